@@ -1,0 +1,248 @@
+// CPU oracle (test infrastructure only): flat C interface for ctypes.
+#include <cstring>
+#include <exception>
+#include <string>
+
+#include "oracle.h"
+#include "solver.h"
+
+using namespace orc;
+
+namespace {
+struct MeshH { Mesh m; Basis1D b; MeshDesc d; };
+struct OpH {
+  MeshH *mh; bool fp32;
+  Operator<double> od; Operator<float> of;
+};
+thread_local std::string g_err;
+}  // namespace
+
+extern "C" {
+
+const char *orc_last_error() { return g_err.c_str(); }
+
+void *orc_mesh_new(int geom, const int *coarse, int level, const double *lo, const double *hi,
+                   double scale, int p, int q, const unsigned char *coarse_active) {
+  try {
+    auto *h = new MeshH();
+    h->d.geometry = geom;
+    for (int k = 0; k < 3; ++k) { h->d.coarse[k] = coarse[k]; h->d.lo[k] = lo[k]; h->d.hi[k] = hi[k]; }
+    h->d.n_refinements = level; h->d.scale = scale; h->d.p = p; h->d.q = q;
+    if (coarse_active) h->d.coarse_active.assign(coarse_active, coarse_active + coarse[0] * coarse[1] * coarse[2]);
+    build_mesh(h->d, level, h->m);
+    h->b.init(p, q);
+    return h;
+  } catch (std::exception &e) { g_err = e.what(); return nullptr; }
+}
+void orc_mesh_free(void *h) { delete (MeshH *)h; }
+void orc_mesh_sizes(void *hh, int *out) {
+  auto *h = (MeshH *)hh;
+  out[0] = h->m.n_cells; out[1] = h->m.n_nodes;
+  for (int k = 0; k < 3; ++k) { out[2 + k] = h->m.nc[k]; out[5 + k] = h->m.nn[k]; }
+  out[8] = (int)h->m.bfaces.size() / 3;
+}
+void orc_mesh_arrays(void *hh, double *X, int *cell_nodes, int *cell_ijk, int *bfaces) {
+  auto *h = (MeshH *)hh;
+  if (X) std::memcpy(X, h->m.X.data(), sizeof(double) * h->m.X.size());
+  if (cell_nodes) std::memcpy(cell_nodes, h->m.cell_nodes.data(), sizeof(int) * h->m.cell_nodes.size());
+  if (cell_ijk) std::memcpy(cell_ijk, h->m.cell_ijk.data(), sizeof(int) * h->m.cell_ijk.size());
+  if (bfaces) std::memcpy(bfaces, h->m.bfaces.data(), sizeof(int) * h->m.bfaces.size());
+}
+double orc_mesh_volume(void *hh) { auto *h = (MeshH *)hh; return mesh_volume(h->m, h->b); }
+void orc_mesh_constraints(void *hh, int n, const int *ids, const int *masks, unsigned char *out) {
+  auto *h = (MeshH *)hh;
+  std::vector<DirichletSpec> bc;
+  for (int i = 0; i < n; ++i) bc.push_back({ids[i], masks[i]});
+  std::vector<uint8_t> m;
+  constrained_dofs(h->m, bc, m);
+  std::memcpy(out, m.data(), m.size());
+}
+void orc_basis(int p, int q, double *nodes, double *qpts, double *qw, double *N, double *D) {
+  Basis1D b; b.init(p, q);
+  std::memcpy(nodes, b.nodes.data(), sizeof(double) * (p + 1));
+  std::memcpy(qpts, b.qpts.data(), sizeof(double) * q);
+  std::memcpy(qw, b.qw.data(), sizeof(double) * q);
+  std::memcpy(N, b.N.data(), sizeof(double) * q * (p + 1));
+  std::memcpy(D, b.D.data(), sizeof(double) * q * (p + 1));
+}
+
+void *orc_op_new(void *mh, int caching, int formulation, int fp32) {
+  try {
+    auto *h = new OpH();
+    h->mh = (MeshH *)mh; h->fp32 = fp32 != 0;
+    if (h->fp32) h->of.initialize(&h->mh->m, &h->mh->b, caching, formulation);
+    else h->od.initialize(&h->mh->m, &h->mh->b, caching, formulation);
+    return h;
+  } catch (std::exception &e) { g_err = e.what(); return nullptr; }
+}
+void orc_op_free(void *h) { delete (OpH *)h; }
+void orc_op_set_material(void *hh, const double *mu, double nu) {
+  auto *h = (OpH *)hh;
+  std::vector<double> m(mu, mu + h->mh->m.n_cells);
+  if (h->fp32) h->of.set_material(m, nu); else h->od.set_material(m, nu);
+}
+void orc_op_set_constraints(void *hh, const unsigned char *mask) {
+  auto *h = (OpH *)hh;
+  std::vector<uint8_t> m(mask, mask + h->mh->m.n_dofs());
+  if (h->fp32) h->of.set_constraints(m); else h->od.set_constraints(m);
+}
+int orc_op_cache(void *hh, const void *u) {
+  auto *h = (OpH *)hh;
+  return h->fp32 ? h->of.cache((const float *)u) : h->od.cache((const double *)u);
+}
+void orc_op_vmult(void *hh, void *dst, const void *src) {
+  auto *h = (OpH *)hh;
+  if (h->fp32) h->of.vmult((float *)dst, (const float *)src);
+  else h->od.vmult((double *)dst, (const double *)src);
+}
+void orc_op_apply_inhom(void *hh, void *dst, const void *g) {
+  auto *h = (OpH *)hh;
+  if (h->fp32) h->of.apply_inhomogeneous((float *)dst, (const float *)g);
+  else h->od.apply_inhomogeneous((double *)dst, (const double *)g);
+}
+void orc_op_diagonal(void *hh, void *diag, void *inv) {
+  auto *h = (OpH *)hh;
+  const size_t n = h->mh->m.n_dofs();
+  if (h->fp32) {
+    h->of.compute_diagonal();
+    if (diag) std::memcpy(diag, h->of.diag.data(), 4 * n);
+    if (inv) std::memcpy(inv, h->of.inv_diag.data(), 4 * n);
+  } else {
+    h->od.compute_diagonal();
+    if (diag) std::memcpy(diag, h->od.diag.data(), 8 * n);
+    if (inv) std::memcpy(inv, h->od.inv_diag.data(), 8 * n);
+  }
+}
+void orc_op_cell_apply(void *hh, int cell, const void *in, void *out) {
+  auto *h = (OpH *)hh;
+  if (h->fp32) h->of.cell_apply(cell, (const float *)in, (float *)out);
+  else h->od.cell_apply(cell, (const double *)in, (double *)out);
+}
+// which: 0 scalar, 1 second scalar, 2 tensor2 (6/qp), 3 tensor4 (36/qp),
+// 4 jinv_cur (9/qp), 5 jxw_cur; returns the element count
+long orc_op_get_table(void *hh, int which, void *out) {
+  auto *h = (OpH *)hh;
+  auto get = [&](auto &op) -> long {
+    const auto *v = which == 0 ? &op.c_scalar : which == 1 ? &op.c_second : which == 2 ? &op.c_t2
+                  : which == 3 ? &op.c_t4 : which == 4 ? &op.jinv_cur : &op.jxw_cur;
+    if (out) std::memcpy(out, v->data(), v->size() * sizeof((*v)[0]));
+    return (long)v->size();
+  };
+  return h->fp32 ? get(h->of) : get(h->od);
+}
+
+double orc_residual(void *mh, const double *mu, double nu, int formulation, const double *u,
+                    int n_neu, const int *neu_ids, const double *neu_ab, double time,
+                    const unsigned char *cmask, double *R) {
+  auto *h = (MeshH *)mh;
+  std::vector<double> m(mu, mu + h->m.n_cells);
+  std::vector<Neumann> neu;
+  for (int i = 0; i < n_neu; ++i) {
+    Neumann nm; nm.id = neu_ids[i];
+    for (int c = 0; c < 3; ++c) { nm.a[c] = neu_ab[6 * i + c]; nm.b[c] = neu_ab[6 * i + 3 + c]; }
+    neu.push_back(nm);
+  }
+  std::vector<uint8_t> cm(cmask, cmask + h->m.n_dofs());
+  return residual(h->m, h->b, m, nu, formulation, u, neu, time, cm, R);
+}
+
+void orc_element_matrix(void *mh, int cell, double mu, double nu, int formulation, const double *u, double *K) {
+  auto *h = (MeshH *)mh;
+  Material mat(mu, nu, formulation);
+  std::vector<double> k;
+  element_matrix(h->m, h->b, cell, mat, u, k);
+  std::memcpy(K, k.data(), sizeof(double) * k.size());
+}
+
+// ------------------------------------------------------------ transfer
+struct TrH { Transfer t; MeshH *c, *f; };
+void *orc_transfer_new(void *coarse, void *fine) {
+  auto *h = new TrH(); h->c = (MeshH *)coarse; h->f = (MeshH *)fine;
+  h->t.build(h->c->m, h->f->m, h->c->b);
+  return h;
+}
+void orc_transfer_free(void *h) { delete (TrH *)h; }
+void orc_transfer_prolongate(void *hh, const unsigned char *ccmask, const double *src, double *dst) {
+  auto *h = (TrH *)hh;
+  std::vector<uint8_t> cm(ccmask, ccmask + h->c->m.n_dofs());
+  std::memset(dst, 0, sizeof(double) * h->f->m.n_dofs());
+  h->t.prolongate_add(h->c->m, cm, src, dst);
+}
+void orc_transfer_restrict(void *hh, const unsigned char *ccmask, const double *src, double *dst) {
+  auto *h = (TrH *)hh;
+  std::vector<uint8_t> cm(ccmask, ccmask + h->c->m.n_dofs());
+  std::memset(dst, 0, sizeof(double) * h->c->m.n_dofs());
+  h->t.restrict_add(h->c->m, cm, src, dst);
+}
+void orc_transfer_interpolate(void *hh, const double *fine_u, double *coarse_u) {
+  auto *h = (TrH *)hh;
+  h->t.interpolate(h->c->m, h->f->m, fine_u, coarse_u);
+}
+
+// ------------------------------------------------------------- Newton
+// Flat parameter block (doubles then ints) so that ctypes can fill it.
+struct orc_newton_params {
+  double lo[3], hi[3], scale, mu, nu, end_time, dt, tol_f, tol_u, tol_f_abs, tol_u_abs, tol_lin,
+      relaxation, smoothing_range, output_point[3];
+  int geometry, coarse[3], n_refinements, p, q, caching, formulation, max_nr, max_it_mult, precond,
+      cheb_degree, cheb_eig_its, coarse_chebyshev, coarse_accurate_eig, level_fp32, has_output_point,
+      n_dirichlet, n_neumann;
+  int dir_ids[8], dir_masks[8];
+  double dir_values[24];
+  int neu_ids[8];
+  double neu_ab[48];
+};
+
+// out_steps: per step [time, newton_its, converged, u0, u1, u2, total_cg_its]
+int orc_newton(const orc_newton_params *P, const double *mu_fine, int *n_cells, int *n_dofs,
+               double *volume, int max_steps, double *out_steps, int *n_steps, double *u_out,
+               int *cg_its_out, int max_cg_entries) {
+  try {
+    NewtonParams prm;
+    prm.mesh.geometry = P->geometry;
+    for (int k = 0; k < 3; ++k) { prm.mesh.coarse[k] = P->coarse[k]; prm.mesh.lo[k] = P->lo[k]; prm.mesh.hi[k] = P->hi[k]; }
+    prm.mesh.n_refinements = P->n_refinements; prm.mesh.scale = P->scale;
+    prm.mesh.p = P->p; prm.mesh.q = P->q;
+    prm.caching = P->caching; prm.formulation = P->formulation;
+    prm.mu = P->mu; prm.nu = P->nu;
+    prm.end_time = P->end_time; prm.dt = P->dt; prm.max_nr = P->max_nr;
+    prm.tol_f = P->tol_f; prm.tol_u = P->tol_u; prm.tol_f_abs = P->tol_f_abs; prm.tol_u_abs = P->tol_u_abs;
+    prm.tol_lin = P->tol_lin; prm.max_it_mult = P->max_it_mult; prm.precond = P->precond;
+    prm.relaxation = P->relaxation; prm.cheb_degree = P->cheb_degree; prm.cheb_eig_its = P->cheb_eig_its;
+    prm.smoothing_range = P->smoothing_range;
+    prm.coarse_chebyshev = P->coarse_chebyshev; prm.coarse_accurate_eig = P->coarse_accurate_eig;
+    prm.level_fp32 = P->level_fp32; prm.has_output_point = P->has_output_point;
+    for (int k = 0; k < 3; ++k) prm.output_point[k] = P->output_point[k];
+    for (int i = 0; i < P->n_dirichlet; ++i) {
+      prm.dirichlet.push_back({P->dir_ids[i], P->dir_masks[i]});
+      prm.dirichlet_value.push_back({P->dir_values[3 * i], P->dir_values[3 * i + 1], P->dir_values[3 * i + 2]});
+    }
+    for (int i = 0; i < P->n_neumann; ++i) {
+      Neumann nm; nm.id = P->neu_ids[i];
+      for (int c = 0; c < 3; ++c) { nm.a[c] = P->neu_ab[6 * i + c]; nm.b[c] = P->neu_ab[6 * i + 3 + c]; }
+      prm.neumann.push_back(nm);
+    }
+    NewtonResult res;
+    if (mu_fine) {
+      Mesh tmp; build_mesh(prm.mesh, prm.mesh.n_refinements, tmp);
+      prm.mu_fine.assign(mu_fine, mu_fine + tmp.n_cells);
+    }
+    int rc = newton_run(prm, res);
+    *n_cells = res.n_cells; *n_dofs = res.n_dofs; *volume = res.volume;
+    *n_steps = (int)res.steps.size();
+    int cgk = 0;
+    for (int s = 0; s < (int)res.steps.size() && s < max_steps; ++s) {
+      const auto &st = res.steps[s];
+      double *o = out_steps + 7 * s;
+      o[0] = st.time; o[1] = st.newton_iterations; o[2] = st.converged;
+      o[3] = st.point_u[0]; o[4] = st.point_u[1]; o[5] = st.point_u[2];
+      int tot = 0;
+      for (int c : st.cg_iterations) { tot += c; if (cg_its_out && cgk < max_cg_entries) cg_its_out[cgk++] = c; }
+      o[6] = tot;
+    }
+    if (u_out && !res.u.empty()) std::memcpy(u_out, res.u.data(), sizeof(double) * res.u.size());
+    return rc;
+  } catch (std::exception &e) { g_err = e.what(); return -1; }
+}
+
+}  // extern "C"
