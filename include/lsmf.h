@@ -1,0 +1,207 @@
+/*
+ * lsmf.h — C ABI of the B200-native matrix-free Neo-Hookean tangent operator
+ * and its GMG-preconditioned CG / Newton driver.
+ *
+ * Drop-in boundary for the hot path of davydden/large-strain-matrix-free:
+ * each entry point names the reference interface it replaces (file:line,
+ * paths inside that project).  All device buffers are caller-owned raw CUDA
+ * device pointers; vectors are FP64 ("double") or FP32 ("float") arrays of
+ * n_dofs = 3 * n_nodes entries, node-major (dof = 3 * node + component).
+ * Every call is asynchronous on the handle's CUDA stream unless it returns a
+ * host value.  Handles are not thread-safe.  No function throws; failures
+ * are reported as lsmf_status codes (lsmf_status_string gives the text and
+ * lsmf_last_error the detail of the most recent failure on this thread).
+ */
+#ifndef LSMF_H
+#define LSMF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  LSMF_OK = 0,
+  LSMF_ERR_INVALID_ARG = 1,
+  LSMF_ERR_UNKNOWN_CACHING = 2,      /* mf_nh_operator.h:439-442 AssertThrow */
+  LSMF_ERR_DETF_NONPOSITIVE = 3,     /* mf_nh_operator.h:477-483 det_F > 0   */
+  LSMF_ERR_NOT_INITIALIZED = 4,
+  LSMF_ERR_CG_NOT_CONVERGED = 5,     /* SolverControl::NoConvergence         */
+  LSMF_ERR_NEWTON_NOT_CONVERGED = 6, /* mf_elasticity.h:2557-2558            */
+  LSMF_ERR_CUDA = 7,
+  LSMF_ERR_TIMEOUT = 8,
+  LSMF_ERR_PRM = 9,                  /* ParameterHandler::parse_input        */
+  LSMF_ERR_UNSUPPORTED = 10,
+  LSMF_ERR_ALLOC = 11
+} lsmf_status;
+
+/* MF caching variants: "MF caching" (mf_elasticity.h:445-450) */
+typedef enum {
+  LSMF_CACHE_SCALAR = 0,
+  LSMF_CACHE_TENSOR2 = 1,
+  LSMF_CACHE_TENSOR4 = 2
+} lsmf_caching;
+
+typedef enum { LSMF_FP64 = 0, LSMF_FP32 = 1 } lsmf_precision;
+
+/* MFMask stage bits (mf_nh_operator.h:74-85) for vmult breakdowns */
+enum {
+  LSMF_MASK_ZERO = 1, LSMF_MASK_MPI = 2, LSMF_MASK_RW = 4, LSMF_MASK_SF = 8, LSMF_MASK_QD = 16,
+  LSMF_MASK_DEFAULT = 31
+};
+
+typedef enum { LSMF_GEOM_BOX = 0, LSMF_GEOM_COOK = 1 } lsmf_geometry;
+
+/* Structured hexahedral mesh description.  coarse[] cells are refined
+ * n_refinements times (levels 0 .. n_refinements).  BOX: [lo,hi] with
+ * boundary ids -x:0 +x:1 -y:2 +y:3 -z:4 +z:5 and 6 on faces next to masked
+ * (void) cells.  COOK: the Cook membrane of mf_elasticity.h:1339-1398
+ * (x in [0,48], y in [0,44] mapped by grid_y_transform, z in [lo[2],hi[2]],
+ * times scale), ids 1 (x=0) and 11 (x=48).  coarse_active (optional,
+ * coarse[0]*coarse[1]*coarse[2] bytes, x fastest) removes coarse cells. */
+typedef struct {
+  int geometry;
+  int coarse[3];
+  int n_refinements;
+  double lo[3], hi[3];
+  double scale;
+  int degree;        /* "Polynomial degree" */
+  int n_q_points_1d; /* "Quadrature order"  */
+  const uint8_t *coarse_active;
+} lsmf_mesh_desc;
+
+typedef struct lsmf_mesh lsmf_mesh;
+typedef struct lsmf_op lsmf_op;
+typedef struct lsmf_gmg lsmf_gmg;
+typedef struct lsmf_problem lsmf_problem;
+
+const char *lsmf_status_string(lsmf_status s);
+const char *lsmf_last_error(void);
+const char *lsmf_version(void);
+
+/* ---- mesh: replaces make_grid + system_setup (mf_elasticity.h:1339-1708)
+ * for the structured meshes of this path; builds every multigrid level. */
+lsmf_status lsmf_mesh_create(const lsmf_mesh_desc *desc, lsmf_mesh **out);
+void lsmf_mesh_destroy(lsmf_mesh *m);
+/* sizes of a level (level = -1: finest) */
+lsmf_status lsmf_mesh_info(const lsmf_mesh *m, int level, int *n_cells, int *n_nodes, int *n_dofs);
+int lsmf_mesh_n_levels(const lsmf_mesh *m);
+/* host copies: X[3*n_nodes], cell_nodes[n_cells*(p+1)^3], cell_ijk[3*n_cells] */
+lsmf_status lsmf_mesh_arrays(const lsmf_mesh *m, int level, double *X, int *cell_nodes, int *cell_ijk);
+/* Dirichlet constraints, the "Dirichlet IDs and component mask" of
+ * mf_elasticity.h:215-248 / make_constraints :2932-3007: n pairs of
+ * (boundary id, component bits).  Applied on every level. */
+lsmf_status lsmf_mesh_set_dirichlet(lsmf_mesh *m, int n, const int *ids, const int *comp_masks);
+/* host copy of the per-dof constrained flags of a level */
+lsmf_status lsmf_mesh_constraint_mask(const lsmf_mesh *m, int level, uint8_t *mask);
+
+/* ---- operator: NeoHookOperator<dim,p,q,number> (mf_nh_operator.h:147-296) */
+/* initialize(): mf_nh_operator.h:394-443 (caching selection, tables sized) */
+lsmf_status lsmf_operator_create(lsmf_mesh *m, int level, lsmf_caching caching, int formulation,
+                                 lsmf_precision precision, lsmf_op **out);
+void lsmf_operator_destroy(lsmf_op *op);
+/* set_material(): mf_nh_operator.h:594-608, generalised to a per-cell shear
+ * modulus (host array, n_cells of the operator's level) and one Poisson
+ * ratio (material.h:82-94 gives kappa, c_1, lambda). */
+lsmf_status lsmf_operator_set_material(lsmf_op *op, const double *mu_per_cell, double nu);
+/* cache(): mf_nh_operator.h:447-592 plus the Eulerian MatrixFree metric of
+ * mf_elasticity.h:1949-1982.  d_displacement: device vector of the
+ * operator's precision, borrowed (must outlive the operator, like :261).
+ * Returns LSMF_ERR_DETF_NONPOSITIVE if det F <= 0 at any quadrature point. */
+lsmf_status lsmf_operator_cache(lsmf_op *op, const void *d_displacement);
+/* vmult<mask>(): mf_nh_operator.h:612-706 (dst = A src; constrained rows
+ * are identity, :702-705).  Tvmult is the same operator (:626-645). */
+lsmf_status lsmf_operator_vmult(lsmf_op *op, void *d_dst, const void *d_src, unsigned mask);
+/* vmult_add(): dst += A src */
+lsmf_status lsmf_operator_vmult_add(lsmf_op *op, void *d_dst, const void *d_src);
+/* compute_diagonal(): mf_nh_operator.h:789-918, 1503-1557 */
+lsmf_status lsmf_operator_compute_diagonal(lsmf_op *op);
+/* get_matrix_diagonal_inverse(): device pointer owned by the operator */
+lsmf_status lsmf_operator_get_diagonal(lsmf_op *op, const void **d_diag, const void **d_inv_diag);
+/* precondition_Jacobi(): dst = omega * D^-1 src (mf_nh_operator.h:348-360) */
+lsmf_status lsmf_operator_precondition_jacobi(lsmf_op *op, void *d_dst, const void *d_src, double omega);
+/* m(), n(), memory_consumption() (mf_nh_operator.h:300-392) */
+int lsmf_operator_m(const lsmf_op *op);
+size_t lsmf_operator_memory_consumption(const lsmf_op *op);
+/* the CUDA stream every operator call is ordered on (cudaStream_t) */
+lsmf_status lsmf_operator_set_stream(lsmf_op *op, void *stream);
+/* copy a cache table to the host for checking: which = 0 scalar / c1,
+ * 1 second scalar, 2 tau/J (6 per qp), 3 tensor4 (36 per qp), 4 Eulerian
+ * inverse Jacobian (9 per qp), 5 Eulerian JxW; layout [cell][qp][comp]
+ * converted to double.  Returns the number of doubles in *count. */
+lsmf_status lsmf_operator_get_table(lsmf_op *op, int which, double *host, size_t *count);
+
+/* ---- geometric multigrid preconditioner (mf_elasticity.h:1712-2241) ---- */
+typedef struct {
+  int caching;              /* level operators' caching */
+  int formulation;
+  lsmf_precision precision; /* LevelNumberType (float in the reference) */
+  int smoother_degree;      /* Chebyshev degree (5 in mf_elasticity.h:2104) */
+  double smoothing_range;   /* 20 */
+  int eig_cg_iterations;    /* "MF Chebyshev number CG iterations" (30) */
+  int coarse_chebyshev;     /* "MF Chebyshev coarse" (true) */
+  int coarse_accurate_eig;  /* "MF Chebyshev coarse accurate eigenvalues" */
+} lsmf_gmg_desc;
+
+lsmf_status lsmf_gmg_create(lsmf_mesh *m, const lsmf_gmg_desc *desc, lsmf_gmg **out);
+void lsmf_gmg_destroy(lsmf_gmg *g);
+lsmf_status lsmf_gmg_set_material(lsmf_gmg *g, const double *mu_per_fine_cell, double nu);
+/* interpolate_to_mg + level cache + diagonal + Chebyshev eigenvalue
+ * estimates (mf_elasticity.h:1929-2113); d_u_fine: FP64 device vector */
+lsmf_status lsmf_gmg_setup(lsmf_gmg *g, const double *d_u_fine);
+/* PreconditionMG::vmult: one V-cycle, dst = M^-1 src (FP64 device vectors) */
+lsmf_status lsmf_gmg_vmult(lsmf_gmg *g, double *d_dst, const double *d_src);
+/* Chebyshev data of a level: eigenvalue estimates, degree, theta, delta */
+lsmf_status lsmf_gmg_level_info(const lsmf_gmg *g, int level, double *out6);
+
+/* ---- CG (SolverCG as driven by solve_linear_system, mf_elasticity.h:3012-3214) */
+typedef struct {
+  int iterations;
+  double residual;
+  int converged;
+} lsmf_solve_info;
+/* Solve A x = b to ||b - A x|| <= tol_abs (x is the initial guess).  precond:
+ * 0 none, 1 Jacobi (omega * D^-1), 2 the given GMG. */
+lsmf_status lsmf_cg_solve(lsmf_op *fine, int precond, double omega, lsmf_gmg *gmg, double *d_x,
+                          const double *d_b, double tol_abs, int max_it, lsmf_solve_info *info);
+
+/* ---- residual (assemble_system rhs part, mf_elasticity.h:2708-2922) ---- */
+/* R = -int tau : grad^s N dV + f_ext, constrained entries zeroed; returns
+ * ||R|| in *norm.  d_mu_cell / traction handled by the problem object. */
+
+/* ---- full problem: .prm driven load stepping (Solid::run) ---- */
+/* Parse a reference-format .prm text (ParameterHandler syntax, keys of
+ * mf_elasticity.h:156-607) plus the additive keys documented in
+ * INTEGRATION.md, build mesh, operators, GMG and loads. */
+lsmf_status lsmf_problem_create(const char *prm_text, lsmf_problem **out);
+void lsmf_problem_destroy(lsmf_problem *p);
+/* per fine cell shear modulus override (host array) */
+lsmf_status lsmf_problem_set_mu(lsmf_problem *p, const double *mu_per_cell);
+lsmf_status lsmf_problem_info(const lsmf_problem *p, int *n_cells, int *n_dofs, double *volume);
+/* Run all load steps (Solid::run, mf_elasticity.h:1187-1235). */
+typedef struct {
+  int n_steps;
+  int newton_iterations[256];   /* per load step */
+  int cg_iterations[256];       /* sum over the Newton steps of a load step */
+  double point_u[256][3];       /* displacement at the first output point */
+  double time_residual, time_setup, time_solve; /* seconds, device-timed */
+} lsmf_newton_info;
+lsmf_status lsmf_problem_run(lsmf_problem *p, lsmf_newton_info *info);
+/* final displacement (host, n_dofs doubles) */
+lsmf_status lsmf_problem_get_solution(const lsmf_problem *p, double *host_u);
+
+/* ---- adjoint gradient (new, no reference counterpart) ----
+ * forward: solve with mu = exp(log_mu) per fine cell; J = 1/2 sum over the
+ * dofs of boundary id `obj_id` of (u - u_target)^2.
+ * backward: K(u)^T lambda = dJ/du with the same GMG-CG, then
+ * dJ/dlog_mu_c = -lambda^T dR_int/dlog_mu_c evaluated cell by cell. */
+lsmf_status lsmf_adjoint_forward(lsmf_problem *p, const double *log_mu_cell, const double *u_target,
+                                 int obj_id, double *J);
+lsmf_status lsmf_adjoint_backward(lsmf_problem *p, double *dJ_dlogmu);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LSMF_H */

@@ -1,0 +1,341 @@
+// Device building blocks of the cell kernels: warp-cooperative sum
+// factorisation and the quadrature-point physics of the Neo-Hookean tangent.
+//
+// Execution model: one warp owns one cell at a time.  Lanes stride over the
+// work items of each tensor-product sweep; intermediate tensors live in a
+// per-warp shared-memory slab, so only __syncwarp() separates the sweeps.
+// Quadrature point q belongs to lane q % 32 (QPL = ceil(Q^3/32) points per
+// lane), so everything per quadrature point stays in registers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "lsmf_internal.h"
+
+namespace lsmf {
+
+enum Variant { VAR_TENSOR4 = 0, VAR_TENSOR2 = 1, VAR_SCALAR_F1 = 2, VAR_SCALAR_F0 = 3 };
+
+// Record layout per cell: [comp][qp]; first 10 components are the Eulerian
+// metric (inverse Jacobian row-major, JxW) in every variant.
+constexpr int C_JINV = 0, C_JXW = 9, C_VAR = 10;
+__host__ __device__ constexpr int variant_ncomp(int v) {
+  return v == VAR_TENSOR4 ? 52 : v == VAR_TENSOR2 ? 18 : 20;
+}
+
+template <int P, int Q>
+struct Tab {
+  double N[Q][P + 1], D[Q][P + 1], w[Q];
+};
+
+template <int P, int Q, typename T>
+struct SF {
+  static constexpr int N1 = P + 1, NN = N1 * N1 * N1, NQ = Q * Q * Q;
+  static constexpr int QPL = (NQ + 31) / 32;   // quadrature points per lane
+  static constexpr int NPL = (NN + 31) / 32;   // nodes per lane
+  static constexpr int NA = 3 * N1 * N1 * Q;   // x-sweep outputs per field
+  static constexpr int NB = 3 * N1 * Q * Q;    // y-sweep outputs per field
+  static constexpr int SZ1 = (3 * NN > 9 * NQ) ? 3 * NN : 9 * NQ;
+  static constexpr int SZ2 = 2 * NA;
+  static constexpr int SZ3 = 3 * NB;
+  static constexpr int SZ = SZ1 + SZ2 + SZ3;   // per-warp slab (elements of T)
+  static constexpr int TAB = 2 * Q * N1;        // sN + sD
+
+  // nodal values V[c][k][j][i] (c*NN + node) -> G[i][c][e] at the owned points
+  static __device__ __forceinline__ void eval(const T *__restrict__ sN, const T *__restrict__ sD,
+                                              const T *V, T *A, T *B, int lane, T G[QPL][3][3]) {
+    for (int it = lane; it < NA; it += 32) {
+      const int qx = it % Q, r = it / Q;
+      const T *v = V + r * N1;
+      T s0 = 0, s1 = 0;
+#pragma unroll
+      for (int i = 0; i < N1; ++i) {
+        const T x = v[i];
+        s0 += sN[qx * N1 + i] * x;
+        s1 += sD[qx * N1 + i] * x;
+      }
+      A[it] = s0;
+      A[NA + it] = s1;
+    }
+    __syncwarp();
+    for (int it = lane; it < NB; it += 32) {
+      const int qx = it % Q, qy = (it / Q) % Q, ck = it / (Q * Q);
+      T s00 = 0, s01 = 0, s10 = 0;
+#pragma unroll
+      for (int j = 0; j < N1; ++j) {
+        const T a0 = A[(ck * N1 + j) * Q + qx], a1 = A[NA + (ck * N1 + j) * Q + qx];
+        const T nn = sN[qy * N1 + j], dd = sD[qy * N1 + j];
+        s00 += nn * a0;
+        s01 += dd * a0;
+        s10 += nn * a1;
+      }
+      B[it] = s00;
+      B[NB + it] = s01;
+      B[2 * NB + it] = s10;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int l = 0; l < QPL; ++l) {
+      const int q = lane + 32 * l;
+      if (q < NQ) {
+        const int qx = q % Q, qy = (q / Q) % Q, qz = q / (Q * Q);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          T gx = 0, gy = 0, gz = 0;
+#pragma unroll
+          for (int k = 0; k < N1; ++k) {
+            const int b = ((c * N1 + k) * Q + qy) * Q + qx;
+            const T nn = sN[qz * N1 + k];
+            gx += nn * B[2 * NB + b];
+            gy += nn * B[NB + b];
+            gz += sD[qz * N1 + k] * B[b];
+          }
+          G[l][c][0] = gx;
+          G[l][c][1] = gy;
+          G[l][c][2] = gz;
+        }
+      }
+    }
+    __syncwarp();
+  }
+
+  // H[i][c][e] at owned points -> nodal values out[c][node] in smem Yout
+  // (= the V region), the transpose of eval().
+  static __device__ __forceinline__ void integrate(const T *__restrict__ sN, const T *__restrict__ sD,
+                                                   const T H[QPL][3][3], T *Hs, T *Y, T *Z, int lane) {
+#pragma unroll
+    for (int l = 0; l < QPL; ++l) {
+      const int q = lane + 32 * l;
+      if (q < NQ) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int e = 0; e < 3; ++e) Hs[(c * 3 + e) * NQ + q] = H[l][c][e];
+      }
+    }
+    __syncwarp();
+    // z: Z[c][k][qy][qx] for the three gradient directions
+    for (int it = lane; it < NB; it += 32) {
+      const int qx = it % Q, qy = (it / Q) % Q, ck = it / (Q * Q);
+      const int c = ck / N1, k = ck % N1;
+      T sx = 0, sy = 0, sz = 0;
+#pragma unroll
+      for (int qz = 0; qz < Q; ++qz) {
+        const int q = (qz * Q + qy) * Q + qx;
+        const T nn = sN[qz * N1 + k];
+        sx += nn * Hs[(c * 3 + 0) * NQ + q];
+        sy += nn * Hs[(c * 3 + 1) * NQ + q];
+        sz += sD[qz * N1 + k] * Hs[(c * 3 + 2) * NQ + q];
+      }
+      Z[it] = sx;
+      Z[NB + it] = sy;
+      Z[2 * NB + it] = sz;
+    }
+    __syncwarp();
+    // y: Yx[c][k][j][qx], Yo[c][k][j][qx]
+    for (int it = lane; it < NA; it += 32) {
+      const int qx = it % Q, j = (it / Q) % N1, ck = it / (Q * N1);
+      T sx = 0, so = 0;
+#pragma unroll
+      for (int qy = 0; qy < Q; ++qy) {
+        const int z = (ck * Q + qy) * Q + qx;
+        const T nn = sN[qy * N1 + j];
+        sx += nn * Z[z];
+        so += sD[qy * N1 + j] * Z[NB + z] + nn * Z[2 * NB + z];
+      }
+      Y[it] = sx;
+      Y[NA + it] = so;
+    }
+    __syncwarp();
+  }
+
+  // final x sweep for node a = (i, j, k): 3 component values
+  static __device__ __forceinline__ void integrate_node(const T *__restrict__ sN, const T *__restrict__ sD,
+                                                        const T *Y, int a, T out[3]) {
+    const int i = a % N1, jk = a / N1;  // jk = k*N1 + j
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int base = ((c * N1 * N1) + jk) * Q;
+      T s = 0;
+#pragma unroll
+      for (int qx = 0; qx < Q; ++qx) s += sD[qx * N1 + i] * Y[base + qx] + sN[qx * N1 + i] * Y[NA + base + qx];
+      out[c] = s;
+    }
+  }
+};
+
+// --------------------------------------------------------------- physics
+// symmetric storage (0,0),(1,1),(2,2),(0,1),(0,2),(1,2)
+__device__ __forceinline__ int sym_i(int I) { return I < 3 ? I : (I == 5 ? 1 : 0); }
+__device__ __forceinline__ int sym_j(int I) { return I < 3 ? I : (I == 3 ? 1 : 2); }
+
+template <typename T>
+__device__ __forceinline__ T det3(const T F[3][3]) {
+  return F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) - F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
+         F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
+}
+template <typename T>
+__device__ __forceinline__ T inv3(const T J[3][3], T Ji[3][3]) {
+  const T d = det3(J);
+  const T id = T(1) / d;
+  Ji[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) * id;
+  Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+  Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+  Ji[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) * id;
+  Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+  Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+  Ji[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) * id;
+  Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+  Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+  return d;
+}
+
+// Per-point state of the scalar variants (computed from the displacement).
+template <typename T>
+struct ScalarState {
+  T F[3][3];
+  T det;
+};
+
+// Q(g) of do_operation_on_cell (mf_nh_operator.h:922-1499) for the point
+// whose record is rec[comp * NQ] (rec already offset by q).
+template <typename T, int VAR, int NQ>
+__device__ __forceinline__ void physics(const T g[3][3], const T *__restrict__ rec, T mu, T lambda, T kappa,
+                                        const ScalarState<T> &st, T Qm[3][3]) {
+  T s[6];
+#pragma unroll
+  for (int I = 0; I < 6; ++I) s[I] = T(0.5) * (g[sym_i(I)][sym_j(I)] + g[sym_j(I)][sym_i(I)]);
+  const T tr = s[0] + s[1] + s[2];
+  if (VAR == VAR_TENSOR4) {
+    // g * (tau/J) + C : sym(g)     (mf_nh_operator.h:1425-1440)
+    T Ts[6];
+#pragma unroll
+    for (int I = 0; I < 6; ++I) Ts[I] = rec[(C_VAR + I) * NQ];
+    T cs[6];
+#pragma unroll
+    for (int I = 0; I < 6; ++I) {
+      T a = 0;
+#pragma unroll
+      for (int J = 0; J < 6; ++J) a += rec[(C_VAR + 6 + I * 6 + J) * NQ] * s[J];
+      cs[I] = a;
+    }
+    const T T00 = Ts[0], T11 = Ts[1], T22 = Ts[2], T01 = Ts[3], T02 = Ts[4], T12 = Ts[5];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      Qm[i][0] = g[i][0] * T00 + g[i][1] * T01 + g[i][2] * T02;
+      Qm[i][1] = g[i][0] * T01 + g[i][1] * T11 + g[i][2] * T12;
+      Qm[i][2] = g[i][0] * T02 + g[i][1] * T12 + g[i][2] * T22;
+    }
+    Qm[0][0] += cs[0]; Qm[1][1] += cs[1]; Qm[2][2] += cs[2];
+    Qm[0][1] += cs[3]; Qm[1][0] += cs[3];
+    Qm[0][2] += cs[4]; Qm[2][0] += cs[4];
+    Qm[1][2] += cs[5]; Qm[2][1] += cs[5];
+  } else if (VAR == VAR_TENSOR2) {
+    // c1 sym(g) + c2 tr(g) I + g * (tau/J)   (mf_nh_operator.h:1401-1424)
+    const T c1 = rec[C_VAR * NQ], c2 = rec[(C_VAR + 1) * NQ];
+    const T T00 = rec[(C_VAR + 2) * NQ], T11 = rec[(C_VAR + 3) * NQ], T22 = rec[(C_VAR + 4) * NQ];
+    const T T01 = rec[(C_VAR + 5) * NQ], T02 = rec[(C_VAR + 6) * NQ], T12 = rec[(C_VAR + 7) * NQ];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      Qm[i][0] = g[i][0] * T00 + g[i][1] * T01 + g[i][2] * T02;
+      Qm[i][1] = g[i][0] * T01 + g[i][1] * T11 + g[i][2] * T12;
+      Qm[i][2] = g[i][0] * T02 + g[i][1] * T12 + g[i][2] * T22;
+    }
+#pragma unroll
+    for (int I = 0; I < 6; ++I) {
+      const int i = sym_i(I), j = sym_j(I);
+      const T v = c1 * s[I] + (I < 3 ? c2 * tr : T(0));
+      Qm[i][j] += v;
+      if (i != j) Qm[j][i] += v;
+    }
+  } else if (VAR == VAR_SCALAR_F1) {
+    // mf_nh_operator.h:1182-1254: tau = mu b - c I, jc = 2c sym + 2 lambda tr I
+    const T c = rec[C_VAR * NQ];
+    T jc[6];
+#pragma unroll
+    for (int I = 0; I < 6; ++I) jc[I] = T(2) * c * s[I] + (I < 3 ? T(2) * lambda * tr : T(0));
+    T tau[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const T b = st.F[i][0] * st.F[j][0] + st.F[i][1] * st.F[j][1] + st.F[i][2] * st.F[j][2];
+        tau[i][j] = mu * b - (i == j ? c : T(0));
+      }
+    const T idet = T(1) / st.det;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        T geo = g[i][0] * tau[0][j] + g[i][1] * tau[1][j] + g[i][2] * tau[2][j];
+        Qm[i][j] = geo;
+      }
+#pragma unroll
+    for (int I = 0; I < 6; ++I) {
+      const int i = sym_i(I), j = sym_j(I);
+      Qm[i][j] += jc[I];
+      if (i != j) Qm[j][i] += jc[I];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) Qm[i][j] *= idet;
+  } else {
+    // formulation 0 (vol/iso split), mf_nh_operator.h:1001-1181
+    const T Jm13 = rec[C_VAR * NQ];
+    const T det_F = st.det;
+    T bbar[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        bbar[i][j] = (st.F[i][0] * st.F[j][0] + st.F[i][1] * st.F[j][1] + st.F[i][2] * st.F[j][2]) * Jm13 * Jm13;
+    const T c_1 = T(0.5) * mu;
+    T tau_bar[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) tau_bar[i][j] = bbar[i][j] * (T(2) * c_1);
+    const T tr_tau_bar = tau_bar[0][0] + tau_bar[1][1] + tau_bar[2][2];
+    const T trd = tr_tau_bar * T(1.0 / 3.0);
+    const T dPsi = (kappa / T(2)) * (det_F - T(1) / det_F);
+    const T dPsi_J = dPsi * det_F;
+    const T d2Psi = (kappa / T(2)) * (T(1) + T(1) / (det_F * det_F));
+    T sym[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) sym[i][j] = T(0.5) * (g[i][j] + g[j][i]);
+    T tis = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) tis += (tau_bar[i][j] - (i == j ? trd : T(0))) * sym[i][j];
+    const T volI = det_F * (dPsi + det_F * d2Psi) * tr;
+    const T two3 = T(2.0 / 3.0);
+    const T idet = T(1) / det_F;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const T tau_iso = tau_bar[i][j] - (i == j ? trd : T(0));
+        T v = sym[i][j] * (-dPsi_J * T(2));
+        if (i == j) v += volI;
+        v += (two3 * tr_tau_bar) * (sym[i][j] - (i == j ? tr * T(1.0 / 3.0) : T(0)));
+        v -= (two3 * tr) * tau_iso;
+        if (i == j) v -= two3 * tis;
+        Qm[i][j] = v;
+      }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const T tau_0j = tau_bar[0][j] + (0 == j ? dPsi_J - trd : T(0));
+        const T tau_1j = tau_bar[1][j] + (1 == j ? dPsi_J - trd : T(0));
+        const T tau_2j = tau_bar[2][j] + (2 == j ? dPsi_J - trd : T(0));
+        const T geo = g[i][0] * tau_0j + g[i][1] * tau_1j + g[i][2] * tau_2j;
+        Qm[i][j] = (Qm[i][j] + geo) * idet;
+      }
+  }
+}
+
+}  // namespace lsmf

@@ -1,0 +1,611 @@
+// sm_100a kernels of the matrix-free tangent operator:
+//   cache_kernel     NeoHookOperator::cache + Eulerian MatrixFree metric
+//   apply_kernel     NeoHookOperator::vmult_add cell loop (gather, sum
+//                    factorisation, quadrature physics, integrate, scatter)
+//   diagonal_kernel  NeoHookOperator::compute_diagonal
+// plus the small element-wise kernels around them.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "cell_kernels.cuh"
+#include "lsmf_internal.h"
+
+namespace lsmf {
+
+namespace {
+
+template <typename T>
+struct KArgs {
+  const int *cell_nodes;
+  int n_cells;
+  int ncomp;
+  T *table;              // cache records (written by cache, read by apply/diag)
+  const T *src;
+  T *dst;
+  const T *u;            // displacement (operator precision)
+  const double *X;       // reference coordinates
+  const double *mu;      // per cell
+  double nu;
+  int *flag;             // device error word
+  unsigned mask;
+};
+
+template <int P, int Q, typename T>
+__device__ __forceinline__ void load_tables(const Tab<P, Q> &tab, T *sN, T *sD) {
+  constexpr int N1 = P + 1;
+  for (int i = threadIdx.x; i < Q * N1; i += blockDim.x) {
+    sN[i] = T(tab.N[i / N1][i % N1]);
+    sD[i] = T(tab.D[i / N1][i % N1]);
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ __forceinline__ void material(double mu_d, double nu, T &mu, T &lambda, T &kappa) {
+  // material.h:82-94
+  mu = T(mu_d);
+  lambda = T((2.0 * mu_d * nu) / (1.0 - 2.0 * nu));
+  kappa = T((2.0 * mu_d * (1.0 + nu)) / (3.0 * (1.0 - 2.0 * nu)));
+}
+
+// gather a 3-component field of a cell into V[c*NN + a]
+template <int NN, typename TS, typename TD>
+__device__ __forceinline__ void gather(const int *__restrict__ cn, const TS *__restrict__ vec, bool zero_constr,
+                                       TD *V, int lane) {
+  for (int a = lane; a < NN; a += 32) {
+    const int packed = __ldg(cn + a);
+    const int node = packed & NODE_MASK;
+    const int cm = zero_constr ? (packed >> NODE_BITS) : 0;
+    const TS *v = vec + 3 * (size_t)node;
+    V[a] = (cm & 1) ? TD(0) : TD(__ldg(v));
+    V[NN + a] = (cm & 2) ? TD(0) : TD(__ldg(v + 1));
+    V[2 * NN + a] = (cm & 4) ? TD(0) : TD(__ldg(v + 2));
+  }
+  __syncwarp();
+}
+
+template <typename T>
+__device__ __forceinline__ void atomic_add(T *a, T v) { atomicAdd(a, v); }
+
+// ------------------------------------------------------------ cache kernel
+template <int P, int Q, typename T, int VAR>
+__global__ void __launch_bounds__(256) cache_kernel(KArgs<T> a, Tab<P, Q> tab) {
+  using S = SF<P, Q, double>;
+  constexpr int NN = S::NN, NQ = S::NQ, QPL = S::QPL;
+  const int WPB = blockDim.x >> 5;
+  extern __shared__ __align__(16) unsigned char smem[];
+  double *sN = (double *)smem, *sD = sN + Q * (P + 1);
+  load_tables<P, Q, double>(tab, sN, sD);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double *slab = sD + Q * (P + 1) + warp * S::SZ;
+  double *V = slab, *A = slab + S::SZ1, *B = A + S::SZ2;
+  const int gw = blockIdx.x * WPB + warp, nw = gridDim.x * WPB;
+  int bad = 0;
+  for (int cell = gw; cell < a.n_cells; cell += nw) {
+    const int *cn = a.cell_nodes + (size_t)cell * NN;
+    double GX[QPL][3][3], GU[QPL][3][3];
+    gather<NN>(cn, a.X, false, V, lane);
+    S::eval(sN, sD, V, A, B, lane, GX);
+    gather<NN>(cn, a.u, false, V, lane);
+    S::eval(sN, sD, V, A, B, lane, GU);
+    const double mu = a.mu[cell];
+    const double lambda = (2.0 * mu * a.nu) / (1.0 - 2.0 * a.nu);
+    T *rec = a.table + (size_t)cell * a.ncomp * NQ;
+#pragma unroll
+    for (int l = 0; l < QPL; ++l) {
+      const int q = lane + 32 * l;
+      if (q >= NQ) continue;
+      const double w = tab.w[q % Q] * tab.w[(q / Q) % Q] * tab.w[q / (Q * Q)];
+      double Jr[3][3], Jc[3][3], Jri[3][3], Jci[3][3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+          Jr[d][e] = GX[l][d][e];
+          Jc[d][e] = GX[l][d][e] + GU[l][d][e];
+        }
+      inv3(Jr, Jri);
+      const double dc = inv3(Jc, Jci);
+      T *r = rec + q;
+#pragma unroll
+      for (int i = 0; i < 9; ++i) r[(C_JINV + i) * NQ] = T(Jci[i / 3][i % 3]);
+      r[C_JXW * NQ] = T(dc * w);
+      // F = I + Grad u (reference configuration, mf_nh_operator.h:462-476)
+      double F[3][3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          F[c][d] = GU[l][c][0] * Jri[0][d] + GU[l][c][1] * Jri[1][d] + GU[l][c][2] * Jri[2][d] + (c == d ? 1.0 : 0.0);
+      const double det_F = det3(F);
+      if (!(det_F > 0.0)) bad = 1;
+      if (VAR == VAR_SCALAR_F0 || VAR == VAR_SCALAR_F1) {
+        const double c = (VAR == VAR_SCALAR_F0) ? pow(det_F, -1.0 / 3.0) : mu - 2.0 * lambda * log(det_F);
+        r[C_VAR * NQ] = T(c);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) r[(C_VAR + 1 + i) * NQ] = T(Jri[i / 3][i % 3]);
+        continue;
+      }
+      const double scalar = mu - 2.0 * lambda * log(det_F);
+      const double idet = 1.0 / det_F;
+      double tau[6];
+#pragma unroll
+      for (int I = 0; I < 6; ++I) {
+        const int i = sym_i(I), j = sym_j(I);
+        const double b = F[i][0] * F[j][0] + F[i][1] * F[j][1] + F[i][2] * F[j][2];
+        tau[I] = mu * b - (i == j ? scalar : 0.0);
+      }
+      if (VAR == VAR_TENSOR2) {
+        r[C_VAR * NQ] = T(scalar * 2.0 * idet);
+        r[(C_VAR + 1) * NQ] = T(2.0 * lambda * idet);
+#pragma unroll
+        for (int I = 0; I < 6; ++I) r[(C_VAR + 2 + I) * NQ] = T(tau[I] * idet);
+      } else {
+#pragma unroll
+        for (int I = 0; I < 6; ++I) r[(C_VAR + I) * NQ] = T(tau[I] * idet);
+        // C = (2c/J) S + (2 lambda/J) I (x) I  (mf_nh_operator.h:542-546)
+        const double ca = scalar * 2.0 * idet, cb = lambda * 2.0 * idet;
+#pragma unroll
+        for (int I = 0; I < 6; ++I)
+#pragma unroll
+          for (int J = 0; J < 6; ++J)
+            r[(C_VAR + 6 + I * 6 + J) * NQ] = T((I == J ? ca : 0.0) + (I < 3 && J < 3 ? cb : 0.0));
+      }
+    }
+    __syncwarp();
+  }
+  if (bad) atomicOr(a.flag, 1);
+}
+
+// ------------------------------------------------------------ apply kernel
+// FULL: all MFMask stages (the production path); otherwise stage bits of
+// a.mask switch RW / SF / QD on and off like vmult<mask> for breakdowns.
+template <int P, int Q, typename T, int VAR, bool FULL>
+__global__ void __launch_bounds__(256) apply_kernel(KArgs<T> a, Tab<P, Q> tab) {
+  using S = SF<P, Q, T>;
+  constexpr int NN = S::NN, NQ = S::NQ, QPL = S::QPL;
+  const int WPB = blockDim.x >> 5;
+  constexpr bool SCALAR = (VAR == VAR_SCALAR_F0 || VAR == VAR_SCALAR_F1);
+  extern __shared__ __align__(16) unsigned char smem[];
+  T *sN = (T *)smem, *sD = sN + Q * (P + 1);
+  load_tables<P, Q, T>(tab, sN, sD);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T *slab = sD + Q * (P + 1) + warp * S::SZ;
+  T *V = slab, *A = slab + S::SZ1, *B = A + S::SZ2;
+  const int gw = blockIdx.x * WPB + warp, nw = gridDim.x * WPB;
+  const bool rw = FULL || (a.mask & LSMF_MASK_RW), sf = FULL || (a.mask & LSMF_MASK_SF),
+             qd = FULL || (a.mask & LSMF_MASK_QD);
+  for (int cell = gw; cell < a.n_cells; cell += nw) {
+    const int *cn = a.cell_nodes + (size_t)cell * NN;
+    const T *rec = a.table + (size_t)cell * a.ncomp * NQ;
+    T G[QPL][3][3], GU[QPL][3][3];
+    if (SCALAR) {
+      if (rw) gather<NN>(cn, a.u, false, V, lane);   // read_dof_values_plain(u)
+      if (sf) S::eval(sN, sD, V, A, B, lane, GU);
+    }
+    if (rw) gather<NN>(cn, a.src, true, V, lane);    // read_dof_values(src)
+    else {
+      for (int i = lane; i < 3 * NN; i += 32) V[i] = T(0);
+      __syncwarp();
+    }
+    if (sf) S::eval(sN, sD, V, A, B, lane, G);
+    else {
+#pragma unroll
+      for (int l = 0; l < QPL; ++l)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int e = 0; e < 3; ++e) G[l][c][e] = T(0);
+    }
+    T mu = 0, lambda = 0, kappa = 0;
+    if (SCALAR) material<T>(a.mu[cell], a.nu, mu, lambda, kappa);
+    T H[QPL][3][3];
+#pragma unroll
+    for (int l = 0; l < QPL; ++l) {
+      const int q = lane + 32 * l;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int e = 0; e < 3; ++e) H[l][c][e] = T(0);
+      if (q >= NQ || !qd) continue;
+      const T *r = rec + q;
+      T Ji[3][3];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) Ji[i / 3][i % 3] = r[(C_JINV + i) * NQ];
+      const T jxw = r[C_JXW * NQ];
+      T g[3][3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) g[c][d] = G[l][c][0] * Ji[0][d] + G[l][c][1] * Ji[1][d] + G[l][c][2] * Ji[2][d];
+      ScalarState<T> st;
+      if (SCALAR) {
+        T Jr[3][3];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) Jr[i / 3][i % 3] = r[(C_VAR + 1 + i) * NQ];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            st.F[c][d] = GU[l][c][0] * Jr[0][d] + GU[l][c][1] * Jr[1][d] + GU[l][c][2] * Jr[2][d] + (c == d ? T(1) : T(0));
+        st.det = det3(st.F);
+      }
+      T Qm[3][3];
+      physics<T, VAR, NQ>(g, r, mu, lambda, kappa, st, Qm);
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int e = 0; e < 3; ++e) H[l][c][e] = (Qm[c][0] * Ji[e][0] + Qm[c][1] * Ji[e][1] + Qm[c][2] * Ji[e][2]) * jxw;
+    }
+    if (sf) {
+      S::integrate(sN, sD, H, V, A, B, lane);
+    } else {
+      for (int i = lane; i < S::SZ2; i += 32) A[i] = T(0);
+      __syncwarp();
+    }
+    if (rw) {
+      for (int an = lane; an < NN; an += 32) {
+        T o[3];
+        S::integrate_node(sN, sD, A, an, o);
+        const int packed = __ldg(cn + an);
+        const int node = packed & NODE_MASK, cm = packed >> NODE_BITS;
+        T *d = a.dst + 3 * (size_t)node;
+        if (!(cm & 1)) atomic_add(d, o[0]);
+        if (!(cm & 2)) atomic_add(d + 1, o[1]);
+        if (!(cm & 4)) atomic_add(d + 2, o[2]);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// --------------------------------------------------------- diagonal kernel
+// diag(a,c) = sum_q JxW n^T B_c n with n = grad_x N_a and
+// B_c[d][l] = Q(e_c (x) e_l)[c][d]: identical to applying the cell operator
+// to unit vectors (mf_nh_operator.h:881-899) and keeping the diagonal entry.
+template <int P, int Q, typename T, int VAR>
+__global__ void __launch_bounds__(128) diagonal_kernel(KArgs<T> a, Tab<P, Q> tab) {
+  using S = SF<P, Q, T>;
+  constexpr int N1 = P + 1, NN = S::NN, NQ = S::NQ, QPL = S::QPL;
+  const int WPB = blockDim.x >> 5;
+  constexpr bool SCALAR = (VAR == VAR_SCALAR_F0 || VAR == VAR_SCALAR_F1);
+  constexpr int SZD = S::SZ + 36 * NQ;
+  extern __shared__ __align__(16) unsigned char smem[];
+  T *sN = (T *)smem, *sD = sN + Q * N1;
+  load_tables<P, Q, T>(tab, sN, sD);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T *slab = sD + Q * N1 + warp * SZD;
+  T *V = slab, *A = slab + S::SZ1, *B = A + S::SZ2;
+  T *Bq = slab + S::SZ;  // [q][27] then [q][9] inverse Jacobian
+  T *Jq = Bq + 27 * NQ;
+  const int gw = blockIdx.x * WPB + warp, nw = gridDim.x * WPB;
+  for (int cell = gw; cell < a.n_cells; cell += nw) {
+    const int *cn = a.cell_nodes + (size_t)cell * NN;
+    const T *rec = a.table + (size_t)cell * a.ncomp * NQ;
+    T GU[QPL][3][3];
+    if (SCALAR) {
+      gather<NN>(cn, a.u, false, V, lane);
+      S::eval(sN, sD, V, A, B, lane, GU);
+    }
+    T mu = 0, lambda = 0, kappa = 0;
+    if (SCALAR) material<T>(a.mu[cell], a.nu, mu, lambda, kappa);
+#pragma unroll
+    for (int l = 0; l < QPL; ++l) {
+      const int q = lane + 32 * l;
+      if (q >= NQ) continue;
+      const T *r = rec + q;
+      const T jxw = r[C_JXW * NQ];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) Jq[q * 9 + i] = r[(C_JINV + i) * NQ];
+      ScalarState<T> st;
+      if (SCALAR) {
+        T Jr[3][3];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) Jr[i / 3][i % 3] = r[(C_VAR + 1 + i) * NQ];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            st.F[c][d] = GU[l][c][0] * Jr[0][d] + GU[l][c][1] * Jr[1][d] + GU[l][c][2] * Jr[2][d] + (c == d ? T(1) : T(0));
+        st.det = det3(st.F);
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int ll = 0; ll < 3; ++ll) {
+          T g[3][3];
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) g[i][j] = (i == c && j == ll) ? T(1) : T(0);
+          T Qm[3][3];
+          physics<T, VAR, NQ>(g, r, mu, lambda, kappa, st, Qm);
+#pragma unroll
+          for (int d = 0; d < 3; ++d) Bq[q * 27 + (c * 3 + d) * 3 + ll] = Qm[c][d] * jxw;
+        }
+    }
+    __syncwarp();
+    for (int an = lane; an < NN; an += 32) {
+      const int ix = an % N1, iy = (an / N1) % N1, iz = an / (N1 * N1);
+      T o[3] = {T(0), T(0), T(0)};
+      for (int q = 0; q < NQ; ++q) {
+        const int qx = q % Q, qy = (q / Q) % Q, qz = q / (Q * Q);
+        const T nx = sN[qx * N1 + ix], ny = sN[qy * N1 + iy], nz = sN[qz * N1 + iz];
+        const T gx = sD[qx * N1 + ix] * ny * nz, gy = nx * sD[qy * N1 + iy] * nz, gz = nx * ny * sD[qz * N1 + iz];
+        const T *J = Jq + q * 9;
+        T n[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) n[d] = gx * J[d] + gy * J[3 + d] + gz * J[6 + d];
+        const T *Bc = Bq + q * 27;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          T s = 0;
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            s += n[d] * (Bc[(c * 3 + d) * 3 + 0] * n[0] + Bc[(c * 3 + d) * 3 + 1] * n[1] + Bc[(c * 3 + d) * 3 + 2] * n[2]);
+          o[c] += s;
+        }
+      }
+      const int packed = __ldg(cn + an);
+      const int node = packed & NODE_MASK, cm = packed >> NODE_BITS;
+      T *d = a.dst + 3 * (size_t)node;
+      if (!(cm & 1)) atomic_add(d, o[0]);
+      if (!(cm & 2)) atomic_add(d + 1, o[1]);
+      if (!(cm & 4)) atomic_add(d + 2, o[2]);
+    }
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------------ element-wise ops
+template <typename T>
+__global__ void constrained_add_kernel(T *dst, const T *src, const int *idx, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int k = idx[i];
+    dst[k] += src[k];
+  }
+}
+template <typename T>
+__global__ void constrained_set_kernel(T *dst, const int *idx, int n, T val) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[idx[i]] = val;
+}
+template <typename T>
+__global__ void invert_kernel(T *inv, const T *d, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    inv[i] = T(1) / d[i];
+}
+template <typename T>
+__global__ void scaled_mul_kernel(T *dst, const T *a, const T *b, T s, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = s * a[i] * b[i];
+}
+
+int g_num_sms = 0;
+int num_sms() {
+  if (!g_num_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  return g_num_sms;
+}
+
+template <int P, int Q>
+Tab<P, Q> make_tab(const Basis &b) {
+  Tab<P, Q> t;
+  for (int k = 0; k < Q; ++k) {
+    for (int i = 0; i <= P; ++i) {
+      t.N[k][i] = b.N[k * (P + 1) + i];
+      t.D[k][i] = b.D[k * (P + 1) + i];
+    }
+    t.w[k] = b.qw[k];
+  }
+  return t;
+}
+
+// grid for a persistent-style launch: a whole number of waves of the SMs
+template <typename K>
+int grid_for(K kernel, int threads, size_t smem, int n_items_per_block_total) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  if (per_sm < 1) per_sm = 1;
+  int g = num_sms() * per_sm;
+  if (g > n_items_per_block_total) g = n_items_per_block_total;
+  return g < 1 ? 1 : g;
+}
+
+// warps per block such that the per-warp slabs fit in ~200 KB of shared memory
+inline int warps_for(size_t slab_bytes, int max_warps) {
+  int w = max_warps;
+  while (w > 1 && slab_bytes * w > 200 * 1024) w >>= 1;
+  return w;
+}
+
+int variant_of(const lsmf_op *op) {
+  if (op->caching == LSMF_CACHE_TENSOR4) return VAR_TENSOR4;
+  if (op->caching == LSMF_CACHE_TENSOR2) return VAR_TENSOR2;
+  return op->formulation == 0 ? VAR_SCALAR_F0 : VAR_SCALAR_F1;
+}
+
+template <typename T>
+KArgs<T> make_args(const lsmf_op *op) {
+  const Level &L = op->L();
+  KArgs<T> a;
+  a.cell_nodes = L.d_cell_nodes.ptr;
+  a.n_cells = L.n_cells;
+  a.ncomp = op->ncomp;
+  a.table = (T *)op->d_table.ptr;
+  a.src = nullptr;
+  a.dst = nullptr;
+  a.u = (const T *)op->d_u;
+  a.X = L.d_X.ptr;
+  a.mu = op->d_mu.ptr;
+  a.nu = op->nu;
+  a.flag = op->d_flag.ptr;
+  a.mask = LSMF_MASK_DEFAULT;
+  return a;
+}
+
+template <int P, int Q, typename T, int VAR>
+lsmf_status run_cache(lsmf_op *op) {
+  auto a = make_args<T>(op);
+  const Tab<P, Q> tab = make_tab<P, Q>(op->mesh->basis);
+  using S = SF<P, Q, double>;
+  const int w = warps_for(sizeof(double) * S::SZ, 8);
+  const size_t smem = sizeof(double) * (S::TAB + w * S::SZ);
+  auto k = cache_kernel<P, Q, T, VAR>;
+  LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int g = grid_for(k, 32 * w, smem, (a.n_cells + w - 1) / w);
+  k<<<g, 32 * w, smem, op->stream>>>(a, tab);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+
+template <int P, int Q, typename T, int VAR>
+lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask) {
+  auto a = make_args<T>(op);
+  a.src = src;
+  a.dst = dst;
+  a.mask = mask;
+  const Tab<P, Q> tab = make_tab<P, Q>(op->mesh->basis);
+  using S = SF<P, Q, T>;
+  const int w = warps_for(sizeof(T) * S::SZ, 8);
+  const size_t smem = sizeof(T) * (S::TAB + w * S::SZ);
+  const bool full = (mask & (LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD)) ==
+                    (LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD);
+  if (full) {
+    auto k = apply_kernel<P, Q, T, VAR, true>;
+    LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int g = grid_for(k, 32 * w, smem, (a.n_cells + w - 1) / w);
+    k<<<g, 32 * w, smem, op->stream>>>(a, tab);
+  } else {
+    auto k = apply_kernel<P, Q, T, VAR, false>;
+    LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int g = grid_for(k, 32 * w, smem, (a.n_cells + w - 1) / w);
+    k<<<g, 32 * w, smem, op->stream>>>(a, tab);
+  }
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+
+template <int P, int Q, typename T, int VAR>
+lsmf_status run_diag(lsmf_op *op, T *diag) {
+  auto a = make_args<T>(op);
+  a.dst = diag;
+  const Tab<P, Q> tab = make_tab<P, Q>(op->mesh->basis);
+  using S = SF<P, Q, T>;
+  const int w = warps_for(sizeof(T) * (S::SZ + 36 * S::NQ), 4);
+  const size_t smem = sizeof(T) * (S::TAB + w * (S::SZ + 36 * S::NQ));
+  auto k = diagonal_kernel<P, Q, T, VAR>;
+  LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int g = grid_for(k, 32 * w, smem, (a.n_cells + w - 1) / w);
+  k<<<g, 32 * w, smem, op->stream>>>(a, tab);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+
+#define LSMF_DISPATCH_PQ(p, q, ...)                                              \
+  [&]() -> lsmf_status {                                                         \
+    if ((p) == 1 && (q) == 2) { constexpr int P_ = 1, Q_ = 2; return __VA_ARGS__; } \
+    if ((p) == 2 && (q) == 3) { constexpr int P_ = 2, Q_ = 3; return __VA_ARGS__; } \
+    if ((p) == 3 && (q) == 4) { constexpr int P_ = 3, Q_ = 4; return __VA_ARGS__; } \
+    if ((p) == 4 && (q) == 5) { constexpr int P_ = 4, Q_ = 5; return __VA_ARGS__; } \
+    set_error("unsupported (degree, n_q_points_1d): only q = p + 1, p = 1..4");   \
+    return LSMF_ERR_UNSUPPORTED;                                                 \
+  }()
+
+#define LSMF_DISPATCH_VAR(v, ...)                                                     \
+  [&]() -> lsmf_status {                                                              \
+    switch (v) {                                                                      \
+      case VAR_TENSOR4: { constexpr int V_ = VAR_TENSOR4; return __VA_ARGS__; }       \
+      case VAR_TENSOR2: { constexpr int V_ = VAR_TENSOR2; return __VA_ARGS__; }       \
+      case VAR_SCALAR_F1: { constexpr int V_ = VAR_SCALAR_F1; return __VA_ARGS__; }   \
+      default: { constexpr int V_ = VAR_SCALAR_F0; return __VA_ARGS__; }             \
+    }                                                                                 \
+  }()
+
+}  // namespace
+
+int table_components(int caching, int formulation) {
+  if (caching == LSMF_CACHE_TENSOR4) return variant_ncomp(VAR_TENSOR4);
+  if (caching == LSMF_CACHE_TENSOR2) return variant_ncomp(VAR_TENSOR2);
+  (void)formulation;
+  return variant_ncomp(VAR_SCALAR_F1);
+}
+
+lsmf_status launch_cache(lsmf_op *op) {
+  const Level &L = op->L();
+  const int v = variant_of(op);
+  LSMF_CUDA(cudaMemsetAsync(op->d_flag.ptr, 0, sizeof(int), op->stream));
+  if (op->precision == LSMF_FP64)
+    return LSMF_DISPATCH_PQ(L.p, L.q, LSMF_DISPATCH_VAR(v, (run_cache<P_, Q_, double, V_>(op))));
+  return LSMF_DISPATCH_PQ(L.p, L.q, LSMF_DISPATCH_VAR(v, (run_cache<P_, Q_, float, V_>(op))));
+}
+
+lsmf_status launch_apply(const lsmf_op *op, void *dst, const void *src, unsigned mask, bool add) {
+  const Level &L = op->L();
+  const int v = variant_of(op);
+  const size_t n = (size_t)L.n_dofs();
+  if (!add && (mask & LSMF_MASK_ZERO)) LSMF_CUDA(cudaMemsetAsync(dst, 0, n * op->elem(), op->stream));
+  lsmf_status s;
+  if (op->precision == LSMF_FP64)
+    s = LSMF_DISPATCH_PQ(L.p, L.q,
+                         LSMF_DISPATCH_VAR(v, (run_apply<P_, Q_, double, V_>(op, (double *)dst, (const double *)src, mask))));
+  else
+    s = LSMF_DISPATCH_PQ(L.p, L.q,
+                         LSMF_DISPATCH_VAR(v, (run_apply<P_, Q_, float, V_>(op, (float *)dst, (const float *)src, mask))));
+  if (s != LSMF_OK) return s;
+  // constrained rows: dst += src (mf_nh_operator.h:702-705)
+  const int nc = (int)L.constrained.size();
+  if (nc && (mask & LSMF_MASK_RW)) {
+    const int g = (nc + 255) / 256 < 4 * num_sms() ? (nc + 255) / 256 : 4 * num_sms();
+    if (op->precision == LSMF_FP64)
+      constrained_add_kernel<double><<<g, 256, 0, op->stream>>>((double *)dst, (const double *)src, L.d_constrained.ptr, nc);
+    else
+      constrained_add_kernel<float><<<g, 256, 0, op->stream>>>((float *)dst, (const float *)src, L.d_constrained.ptr, nc);
+    LSMF_CUDA(cudaGetLastError());
+  }
+  return LSMF_OK;
+}
+
+lsmf_status launch_diagonal(lsmf_op *op) {
+  const Level &L = op->L();
+  const int v = variant_of(op);
+  const size_t n = (size_t)L.n_dofs();
+  LSMF_CUDA(cudaMemsetAsync(op->d_diag.ptr, 0, n * op->elem(), op->stream));
+  lsmf_status s;
+  if (op->precision == LSMF_FP64)
+    s = LSMF_DISPATCH_PQ(L.p, L.q, LSMF_DISPATCH_VAR(v, (run_diag<P_, Q_, double, V_>(op, (double *)op->d_diag.ptr))));
+  else
+    s = LSMF_DISPATCH_PQ(L.p, L.q, LSMF_DISPATCH_VAR(v, (run_diag<P_, Q_, float, V_>(op, (float *)op->d_diag.ptr))));
+  if (s != LSMF_OK) return s;
+  const int nc = (int)L.constrained.size();
+  const int g = 4 * num_sms();
+  if (op->precision == LSMF_FP64) {
+    if (nc) constrained_set_kernel<double><<<g, 256, 0, op->stream>>>((double *)op->d_diag.ptr, L.d_constrained.ptr, nc, 1.0);
+    invert_kernel<double><<<g, 256, 0, op->stream>>>((double *)op->d_inv_diag.ptr, (const double *)op->d_diag.ptr, n);
+  } else {
+    if (nc) constrained_set_kernel<float><<<g, 256, 0, op->stream>>>((float *)op->d_diag.ptr, L.d_constrained.ptr, nc, 1.0f);
+    invert_kernel<float><<<g, 256, 0, op->stream>>>((float *)op->d_inv_diag.ptr, (const float *)op->d_diag.ptr, n);
+  }
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+
+lsmf_status launch_jacobi(const lsmf_op *op, void *dst, const void *src, double omega) {
+  const size_t n = (size_t)op->L().n_dofs();
+  const int g = 4 * num_sms();
+  if (op->precision == LSMF_FP64)
+    scaled_mul_kernel<double><<<g, 256, 0, op->stream>>>((double *)dst, (const double *)op->d_inv_diag.ptr,
+                                                         (const double *)src, omega, n);
+  else
+    scaled_mul_kernel<float><<<g, 256, 0, op->stream>>>((float *)dst, (const float *)op->d_inv_diag.ptr,
+                                                        (const float *)src, (float)omega, n);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+
+}  // namespace lsmf

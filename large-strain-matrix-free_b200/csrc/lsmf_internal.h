@@ -1,0 +1,152 @@
+// Internal data model of liblsmf: host-side mesh hierarchy, device buffers,
+// operator state.  Device layouts (HBM):
+//   cell_nodes  int32 [n_cells][(p+1)^3], node id | (constrained comps << 29)
+//   X           double [n_nodes][3] reference node coordinates
+//   vectors     Number [n_nodes][3] (dof = 3*node + comp)
+//   cache table Number [n_cells][n_comp][Q^3] (one contiguous record per cell)
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/lsmf.h"
+
+namespace lsmf {
+
+void set_error(const std::string &msg);
+
+#define LSMF_CUDA(call)                                                       \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess) {                                                  \
+      ::lsmf::set_error(std::string(#call) + ": " + cudaGetErrorString(e_));  \
+      return LSMF_ERR_CUDA;                                                   \
+    }                                                                         \
+  } while (0)
+#define LSMF_TRY(call)                       \
+  do {                                       \
+    lsmf_status s_ = (call);                 \
+    if (s_ != LSMF_OK) return s_;            \
+  } while (0)
+
+constexpr int NODE_BITS = 29;
+constexpr int NODE_MASK = (1 << NODE_BITS) - 1;
+
+// 1D Lagrange basis on Gauss-Lobatto nodes at Gauss points on [0,1].
+struct Basis {
+  int p = 0, q = 0;
+  std::vector<double> nodes, qpts, qw, N, D;  // N, D: [q][p+1]
+  void init(int p, int q);
+  void eval(double x, double *val, double *der) const;
+};
+
+template <typename T>
+struct DevBuf {
+  T *ptr = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr; n = 0;
+  }
+  lsmf_status alloc(size_t count) {
+    if (count == n && ptr) return LSMF_OK;
+    release();
+    if (count == 0) return LSMF_OK;
+    cudaError_t e = cudaMalloc((void **)&ptr, count * sizeof(T));
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      return LSMF_ERR_ALLOC;
+    }
+    n = count;
+    return LSMF_OK;
+  }
+  lsmf_status upload(const T *h, size_t count) {
+    LSMF_TRY(alloc(count));
+    if (count) LSMF_CUDA(cudaMemcpy(ptr, h, count * sizeof(T), cudaMemcpyHostToDevice));
+    return LSMF_OK;
+  }
+};
+
+// One level of the structured hierarchy.
+struct Level {
+  int p = 2, q = 3;
+  int nc[3] = {0, 0, 0}, nn[3] = {0, 0, 0};
+  int n_cells = 0, n_nodes = 0;
+  std::vector<int> lattice_to_node, node_lattice, cell_of_lattice;
+  std::vector<double> X;
+  std::vector<int> cell_nodes;  // raw node ids
+  std::vector<int> cell_ijk;
+  std::vector<int> bfaces;      // (cell, face, id)
+  std::vector<uint8_t> cmask;   // per dof
+  std::vector<int> constrained;
+  // device
+  DevBuf<int> d_cell_nodes;     // packed with constraint bits
+  DevBuf<double> d_X;
+  DevBuf<int> d_constrained;
+  // cell colouring (8 colours) for deterministic scatter paths
+  int ncn() const { return (p + 1) * (p + 1) * (p + 1); }
+  int nq() const { return q * q * q; }
+  int n_dofs() const { return 3 * n_nodes; }
+};
+
+// Cell-wise transfer from level l-1 to level l.
+struct TransferMap {
+  std::vector<int> fine_nodes;   // per coarse cell (2p+1)^3
+  std::vector<double> weight;    // per fine node
+  std::vector<double> P1;        // (2p+1) x (p+1)
+  DevBuf<int> d_fine_nodes;
+  DevBuf<double> d_weight;
+  // interpolation of the fine displacement onto the coarse nodes
+  std::vector<int> interp_fine_cell;   // per coarse node: fine cell
+  std::vector<double> interp_xi;       // per coarse node: 3 local coords in that fine cell
+  DevBuf<int> d_interp_cell;
+  DevBuf<double> d_interp_w;           // per coarse node: (p+1)^3 weights
+};
+
+}  // namespace lsmf
+
+struct lsmf_mesh {
+  lsmf_mesh_desc desc{};
+  std::vector<uint8_t> coarse_active;
+  lsmf::Basis basis;
+  std::vector<lsmf::Level *> levels;          // 0 = coarsest
+  std::vector<lsmf::TransferMap *> transfer;  // transfer[l] : l-1 -> l (l>=1)
+  std::vector<int> dir_ids, dir_masks;
+  ~lsmf_mesh();
+};
+
+struct lsmf_op {
+  lsmf_mesh *mesh = nullptr;
+  int level = 0;
+  int caching = LSMF_CACHE_TENSOR4, formulation = 1;
+  lsmf_precision precision = LSMF_FP64;
+  int ncomp = 0;                     // table components per qp
+  double nu = 0.3;
+  std::vector<double> mu_host;
+  lsmf::DevBuf<double> d_mu;         // per cell
+  lsmf::DevBuf<char> d_table;        // [cell][ncomp][nq] of Number
+  lsmf::DevBuf<char> d_diag, d_inv_diag;
+  lsmf::DevBuf<int> d_flag;          // device error word
+  const void *d_u = nullptr;         // borrowed displacement
+  bool cached = false, have_diag = false;
+  cudaStream_t stream = 0;
+  size_t elem() const { return precision == LSMF_FP64 ? 8 : 4; }
+  lsmf::Level &L() const { return *mesh->levels[level]; }
+};
+
+namespace lsmf {
+// kernels.cu launchers
+lsmf_status launch_cache(lsmf_op *op);
+lsmf_status launch_apply(const lsmf_op *op, void *dst, const void *src, unsigned mask, bool add);
+lsmf_status launch_diagonal(lsmf_op *op);
+lsmf_status upload_basis_tables(const Basis &b);
+int table_components(int caching, int formulation);
+}  // namespace lsmf

@@ -1,0 +1,278 @@
+"""Python host mirror of the reference's NeoHookOperator surface over liblsmf.
+
+The product is liblsmf.so (hand-written sm_100a kernels + host C++ behind
+the C ABI of include/lsmf.h).  This module only binds that ABI with ctypes,
+using torch CUDA tensors as device buffers (plumbing): method names and
+argument meanings follow NeoHookOperator (mf_nh_operator.h:147-296) —
+initialize / set_material / cache / vmult / vmult_add / Tvmult /
+compute_diagonal / get_matrix_diagonal_inverse / precondition_Jacobi / el /
+m / n / memory_consumption / clear.  Errors raise LsmfError carrying the
+lsmf_status.  There is no CPU fallback: without the library or a GPU every
+call fails loudly.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblsmf.so")
+
+CACHING = {"scalar": 0, "tensor2": 1, "tensor4": 2}
+GEOM = {"box": 0, "cook": 1}
+MASK_ZERO, MASK_MPI, MASK_RW, MASK_SF, MASK_QD, MASK_DEFAULT = 1, 2, 4, 8, 16, 31
+
+
+class LsmfError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("lsmf status %d: %s" % (status, msg))
+        self.status = status
+
+
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("geometry", ctypes.c_int), ("coarse", ctypes.c_int * 3), ("n_refinements", ctypes.c_int),
+                ("lo", ctypes.c_double * 3), ("hi", ctypes.c_double * 3), ("scale", ctypes.c_double),
+                ("degree", ctypes.c_int), ("n_q_points_1d", ctypes.c_int),
+                ("coarse_active", ctypes.c_void_p)]
+
+
+class GmgDesc(ctypes.Structure):
+    _fields_ = [("caching", ctypes.c_int), ("formulation", ctypes.c_int), ("precision", ctypes.c_int),
+                ("smoother_degree", ctypes.c_int), ("smoothing_range", ctypes.c_double),
+                ("eig_cg_iterations", ctypes.c_int), ("coarse_chebyshev", ctypes.c_int),
+                ("coarse_accurate_eig", ctypes.c_int)]
+
+
+class SolveInfo(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("residual", ctypes.c_double), ("converged", ctypes.c_int)]
+
+
+class NewtonInfo(ctypes.Structure):
+    _fields_ = [("n_steps", ctypes.c_int), ("newton_iterations", ctypes.c_int * 256),
+                ("cg_iterations", ctypes.c_int * 256), ("point_u", (ctypes.c_double * 3) * 256),
+                ("time_residual", ctypes.c_double), ("time_setup", ctypes.c_double),
+                ("time_solve", ctypes.c_double)]
+
+
+_lib = None
+vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+
+# every function of include/lsmf.h: name -> (restype, argtypes)
+SIGNATURES = {
+    "lsmf_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "lsmf_last_error": (ctypes.c_char_p, []),
+    "lsmf_version": (ctypes.c_char_p, []),
+    "lsmf_mesh_create": (ctypes.c_int, [ctypes.POINTER(MeshDesc), ctypes.POINTER(vp)]),
+    "lsmf_mesh_destroy": (None, [vp]),
+    "lsmf_mesh_info": (ctypes.c_int, [vp, ctypes.c_int, ip, ip, ip]),
+    "lsmf_mesh_n_levels": (ctypes.c_int, [vp]),
+    "lsmf_mesh_arrays": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp]),
+    "lsmf_mesh_set_dirichlet": (ctypes.c_int, [vp, ctypes.c_int, ip, ip]),
+    "lsmf_mesh_constraint_mask": (ctypes.c_int, [vp, ctypes.c_int, vp]),
+    "lsmf_operator_create": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(vp)]),
+    "lsmf_operator_destroy": (None, [vp]),
+    "lsmf_operator_set_material": (ctypes.c_int, [vp, dp, ctypes.c_double]),
+    "lsmf_operator_cache": (ctypes.c_int, [vp, vp]),
+    "lsmf_operator_vmult": (ctypes.c_int, [vp, vp, vp, ctypes.c_uint]),
+    "lsmf_operator_vmult_add": (ctypes.c_int, [vp, vp, vp]),
+    "lsmf_operator_compute_diagonal": (ctypes.c_int, [vp]),
+    "lsmf_operator_get_diagonal": (ctypes.c_int, [vp, ctypes.POINTER(vp), ctypes.POINTER(vp)]),
+    "lsmf_operator_precondition_jacobi": (ctypes.c_int, [vp, vp, vp, ctypes.c_double]),
+    "lsmf_operator_m": (ctypes.c_int, [vp]),
+    "lsmf_operator_memory_consumption": (ctypes.c_size_t, [vp]),
+    "lsmf_operator_set_stream": (ctypes.c_int, [vp, vp]),
+    "lsmf_operator_get_table": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.POINTER(ctypes.c_size_t)]),
+    "lsmf_gmg_create": (ctypes.c_int, [vp, ctypes.POINTER(GmgDesc), ctypes.POINTER(vp)]),
+    "lsmf_gmg_destroy": (None, [vp]),
+    "lsmf_gmg_set_material": (ctypes.c_int, [vp, dp, ctypes.c_double]),
+    "lsmf_gmg_setup": (ctypes.c_int, [vp, vp]),
+    "lsmf_gmg_vmult": (ctypes.c_int, [vp, vp, vp]),
+    "lsmf_gmg_level_info": (ctypes.c_int, [vp, ctypes.c_int, dp]),
+    "lsmf_cg_solve": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, vp, vp, vp, ctypes.c_double,
+                                     ctypes.c_int, ctypes.POINTER(SolveInfo)]),
+    "lsmf_problem_create": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(vp)]),
+    "lsmf_problem_destroy": (None, [vp]),
+    "lsmf_problem_set_mu": (ctypes.c_int, [vp, dp]),
+    "lsmf_problem_info": (ctypes.c_int, [vp, ip, ip, dp]),
+    "lsmf_problem_run": (ctypes.c_int, [vp, ctypes.POINTER(NewtonInfo)]),
+    "lsmf_problem_get_solution": (ctypes.c_int, [vp, dp]),
+    "lsmf_adjoint_forward": (ctypes.c_int, [vp, dp, dp, ctypes.c_int, dp]),
+    "lsmf_adjoint_backward": (ctypes.c_int, [vp, dp]),
+}
+
+
+def lib():
+    """Load liblsmf.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise LsmfError(-1, "liblsmf.so not built: run large-strain-matrix-free_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name, None)
+            if f is not None:
+                f.restype, f.argtypes = res, args
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != 0:
+        raise LsmfError(status, "%s: %s" % (lib().lsmf_status_string(status).decode(),
+                                            lib().lsmf_last_error().decode()))
+
+
+def _dptr(t):
+    import torch
+    if not isinstance(t, torch.Tensor) or not t.is_cuda or not t.is_contiguous():
+        raise LsmfError(1, "device buffers must be contiguous torch CUDA tensors")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Mesh:
+    """Structured hex mesh hierarchy (levels 0..n_refinements)."""
+
+    def __init__(self, geometry="box", coarse=(1, 1, 1), n_refinements=0, lo=(0, 0, 0), hi=(1, 1, 1),
+                 scale=1.0, degree=2, n_q_points_1d=None, coarse_active=None):
+        d = MeshDesc()
+        d.geometry = GEOM[geometry] if isinstance(geometry, str) else int(geometry)
+        for k in range(3):
+            d.coarse[k], d.lo[k], d.hi[k] = coarse[k], lo[k], hi[k]
+        d.n_refinements, d.scale, d.degree = n_refinements, scale, degree
+        d.n_q_points_1d = degree + 1 if n_q_points_1d is None else n_q_points_1d
+        self._mask = None
+        if coarse_active is not None:
+            self._mask = np.ascontiguousarray(coarse_active, dtype=np.uint8)
+            d.coarse_active = self._mask.ctypes.data
+        h = vp()
+        check(lib().lsmf_mesh_create(ctypes.byref(d), ctypes.byref(h)))
+        self.h = h
+        self.degree = degree
+        self.n_levels = lib().lsmf_mesh_n_levels(h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().lsmf_mesh_destroy(self.h)
+            self.h = None
+
+    def info(self, level=-1):
+        nc, nn, nd = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().lsmf_mesh_info(self.h, level, ctypes.byref(nc), ctypes.byref(nn), ctypes.byref(nd)))
+        return nc.value, nn.value, nd.value
+
+    def arrays(self, level=-1):
+        nc, nn, _ = self.info(level)
+        X = np.zeros((nn, 3))
+        cn = np.zeros((nc, (self.degree + 1) ** 3), dtype=np.int32)
+        ijk = np.zeros((nc, 3), dtype=np.int32)
+        check(lib().lsmf_mesh_arrays(self.h, level, X.ctypes.data, cn.ctypes.data, ijk.ctypes.data))
+        return X, cn, ijk
+
+    def set_dirichlet(self, specs):
+        """specs: [(boundary_id, component_bits), ...]"""
+        ids = np.array([s[0] for s in specs] or [0], dtype=np.int32)
+        masks = np.array([s[1] for s in specs] or [0], dtype=np.int32)
+        check(lib().lsmf_mesh_set_dirichlet(self.h, len(specs), ids.ctypes.data_as(ip), masks.ctypes.data_as(ip)))
+
+    def constraint_mask(self, level=-1):
+        _, _, nd = self.info(level)
+        m = np.zeros(nd, dtype=np.uint8)
+        check(lib().lsmf_mesh_constraint_mask(self.h, level, m.ctypes.data))
+        return m
+
+
+class NeoHookOperator:
+    """initialize(): choose caching (scalar / tensor2 / tensor4) and precision."""
+
+    def __init__(self, mesh, caching="tensor4", formulation=1, precision="fp64", level=-1):
+        self.mesh = mesh
+        self.fp32 = precision in ("fp32", "float", 1)
+        h = vp()
+        cach = CACHING[caching] if isinstance(caching, str) else int(caching)
+        check(lib().lsmf_operator_create(mesh.h, level, cach, formulation, 1 if self.fp32 else 0, ctypes.byref(h)))
+        self.h = h
+        self.level = level
+        self._u = None
+
+    def clear(self):
+        if getattr(self, "h", None):
+            lib().lsmf_operator_destroy(self.h)
+            self.h = None
+
+    __del__ = clear
+
+    @property
+    def dtype(self):
+        import torch
+        return torch.float32 if self.fp32 else torch.float64
+
+    def m(self):
+        return lib().lsmf_operator_m(self.h)
+
+    n = m
+
+    def set_material(self, mu_per_cell, nu):
+        nc, _, _ = self.mesh.info(self.level)
+        mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu_per_cell, dtype=np.float64), (nc,)))
+        check(lib().lsmf_operator_set_material(self.h, mu.ctypes.data_as(dp), nu))
+
+    def cache(self, u):
+        """u: device tensor of the operator's precision (borrowed)."""
+        self._u = u
+        check(lib().lsmf_operator_cache(self.h, _dptr(u)))
+
+    def vmult(self, dst, src, mask=MASK_DEFAULT):
+        check(lib().lsmf_operator_vmult(self.h, _dptr(dst), _dptr(src), mask))
+
+    def vmult_add(self, dst, src):
+        check(lib().lsmf_operator_vmult_add(self.h, _dptr(dst), _dptr(src)))
+
+    Tvmult = vmult
+    Tvmult_add = vmult_add
+
+    def compute_diagonal(self):
+        check(lib().lsmf_operator_compute_diagonal(self.h))
+
+    def _diag_tensors(self):
+        d, inv = vp(), vp()
+        check(lib().lsmf_operator_get_diagonal(self.h, ctypes.byref(d), ctypes.byref(inv)))
+        n = self.m()
+        return [device_view(p.value, n, self.fp32).clone() for p in (d, inv)]
+
+    def get_matrix_diagonal_inverse(self):
+        return self._diag_tensors()[1]
+
+    def get_matrix_diagonal(self):
+        return self._diag_tensors()[0]
+
+    def el(self, row, col):
+        if row != col:
+            raise LsmfError(10, "el() is only defined on the diagonal")
+        return float(self.get_matrix_diagonal()[row])
+
+    def precondition_Jacobi(self, dst, src, omega):
+        check(lib().lsmf_operator_precondition_jacobi(self.h, _dptr(dst), _dptr(src), omega))
+
+    def memory_consumption(self):
+        return lib().lsmf_operator_memory_consumption(self.h)
+
+    def table(self, which):
+        cnt = ctypes.c_size_t()
+        check(lib().lsmf_operator_get_table(self.h, which, None, ctypes.byref(cnt)))
+        out = np.zeros(cnt.value)
+        check(lib().lsmf_operator_get_table(self.h, which, out.ctypes.data_as(dp), ctypes.byref(cnt)))
+        return out
+
+
+class _DevArray:
+    """__cuda_array_interface__ view of a device buffer owned by liblsmf."""
+
+    def __init__(self, ptr, n, fp32):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f4" if fp32 else "<f8",
+                                         "data": (ptr, False), "version": 3, "strides": None}
+
+
+def device_view(ptr, n, fp32=False):
+    import torch
+    return torch.as_tensor(_DevArray(ptr, n, fp32), device="cuda")
