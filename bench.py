@@ -1,0 +1,369 @@
+"""Benchmark of the matrix-free Neo-Hookean tangent operator on B200.
+
+Workload (one "step"): one tangent vmult, tensor4 caching, FP64, on the
+64^3-cell Q2 unit cube (6,440,067 DoFs): per-cell mu drawn from {1, 10} by
+seed, nu = 0.3, bottom face clamped, a seeded smooth displacement field
+bounded by 0.01 (det F > 0.5 checked) and a seeded source vector
+uniform in [-1, 1].  The cache tables (2.9 GB) are larger than L2, so no
+L2 flush is needed between timed steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl lsmf|reference]
+
+N > 1 runs N independent replicas (one per GPU, launched with torchrun):
+the operator has no exchange step in this configuration.  Rank 0 prints one
+JSON line.  --impl reference times the CPU implementation of the same
+operator (the oracle restatement of the reference, OpenMP over all host
+cores) on the same configuration.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "large-strain-matrix-free_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+N_CELLS_1D = 64
+DEGREE = 2
+NU = 0.3
+METRIC = "Tangent vmult GDoF/s & Newton-step time, FP32-GMG vs FP64, same 1e-8 residual"
+
+
+def alg_bytes(variant, S, n_nodes, n_qp, n_cells):
+    """Algorithmic bytes per vmult (values counted once, index maps excluded):
+    scalar S(9N + 11Q + 10C), tensor2 S(6N + 18Q), tensor4 S(6N + 52Q)."""
+    if variant == "tensor4":
+        return S * (6 * n_nodes + 52 * n_qp)
+    if variant == "tensor2":
+        return S * (6 * n_nodes + 18 * n_qp)
+    return S * (9 * n_nodes + 11 * n_qp + 10 * n_cells)
+
+
+def smooth_field(X, seed, amp=0.01, modes=3):
+    """Seeded smooth displacement, |u_c| <= amp: sums of sines of low wave numbers."""
+    rng = np.random.default_rng(seed)
+    u = np.zeros_like(X)
+    for c in range(3):
+        for _ in range(modes):
+            k = rng.integers(1, 3, size=3)
+            a = rng.uniform(-1, 1) * amp / modes
+            ph = rng.uniform(0, 2 * np.pi)
+            u[:, c] += a * np.sin(np.pi * (X @ k) + ph)
+    return u
+
+
+def min_det_f(seed, amp=0.01, modes=3, n=24):
+    """Smallest det(I + grad u) of smooth_field on a sample grid (analytic gradient)."""
+    rng = np.random.default_rng(seed)
+    g = np.linspace(0, 1, n)
+    X = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    G = np.zeros((X.shape[0], 3, 3))
+    for c in range(3):
+        for _ in range(modes):
+            k = rng.integers(1, 3, size=3)
+            a = rng.uniform(-1, 1) * amp / modes
+            ph = rng.uniform(0, 2 * np.pi)
+            G[:, c, :] += (a * np.pi * np.cos(np.pi * (X @ k) + ph))[:, None] * k[None, :]
+    F = G + np.eye(3)[None]
+    return float(np.linalg.det(F).min())
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([s.strip() for s in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(s[0]) for s in self.samples if len(s) >= 8 and s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if len(s) >= 8 and s[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            if len(s) < 8:
+                continue
+            for nm, v in zip(names, s[4:8]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def read_traffic():
+    """DRAM bytes per launch of the tensor4 FP64 apply kernel from the
+    committed ncu summary (profiles/apply_tensor4_fp64_64cube.md)."""
+    p = os.path.join(ROOT, "profiles", "apply_tensor4_fp64_64cube.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------- CPU (oracle)
+def cpu_vmult_rate(n_cells_1d, variant, fp32, steps, seed=1234):
+    """Time the oracle's OpenMP vmult (the CPU implementation of the same
+    operator) on the same mesh and inputs; returns (GDoF/s, seconds, n_dofs)."""
+    import oracle as O
+    m = O.Mesh(O.GEOM_BOX, (n_cells_1d,) * 3, 0, (0, 0, 0), (1, 1, 1), 1.0, DEGREE, DEGREE + 1)
+    rng = np.random.default_rng(seed)
+    mu = rng.choice([1.0, 10.0], size=m.n_cells)
+    u = smooth_field(m.X, seed).reshape(-1)
+    src = np.random.default_rng(seed + 1).uniform(-1, 1, m.n_dofs)
+    op = O.Operator(m, variant, 1, fp32=fp32)
+    op.set_material(mu, NU)
+    op.set_constraints(m.constraints([(4, 7)]))
+    op.cache(u.astype(np.float32) if fp32 else u)
+    op.vmult(src)  # warm-up
+    ts = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        op.vmult(src)
+        ts.append(time.perf_counter() - t)
+    t = float(np.median(ts))
+    return m.n_dofs / t / 1e9, t, m.n_dofs
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    rate, t, n_dofs = cpu_vmult_rate(args.cells, "tensor4", False, max(1, args.steps))
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "GDoF/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": "tangent vmult, tensor4 caching, FP64, %d^3-cell Q2 unit cube" % args.cells,
+                       "n_dofs": n_dofs, "parallelism": "OpenMP over host cores"},
+            "cpu_baseline": {"value": rate, "unit": "GDoF/s", "cores": threads, "kind": "port",
+                             "sample": "%d vmults of the full %d^3 Q2 workload (median)" % (args.steps, args.cells)},
+            "e2e": {"value": rate, "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU (lsmf)
+def run_lsmf(args):
+    import torch
+    import lsmf
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    seed = 1234
+    assert min_det_f(seed) > 0.5
+    mesh = lsmf.Mesh("box", (args.cells,) * 3, 0, degree=DEGREE)
+    mesh.set_dirichlet([(4, 7)])
+    n_cells, n_nodes, n_dofs = mesh.info()
+    X, _, _ = mesh.arrays()
+    rng = np.random.default_rng(seed)
+    mu = rng.choice([1.0, 10.0], size=n_cells)
+    u_h = smooth_field(X, seed).reshape(-1)
+    src_h = np.random.default_rng(seed + 1).uniform(-1, 1, n_dofs)
+    n_qp = n_cells * (DEGREE + 1) ** 3
+    u64 = torch.tensor(u_h, device="cuda")
+    u32 = u64.float()
+    src64 = torch.tensor(src_h, device="cuda")
+    src32 = src64.float()
+
+    def make(variant, prec):
+        op = lsmf.NeoHookOperator(mesh, variant, 1, prec)
+        op.set_material(mu, NU)
+        op.cache(u64 if prec == "fp64" else u32)
+        return op
+
+    op = make("tensor4", "fp64")
+    dst = torch.empty_like(src64)
+    stream = torch.cuda.current_stream()
+    lib = lsmf.lib()
+    lib.lsmf_operator_set_stream(op.h, lsmf.vp(stream.cuda_stream))
+
+    for _ in range(args.warmup):
+        op.vmult(dst, src64)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        op.vmult(dst, src64)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_ms = e0.elapsed_time(e1)
+    # kernel-level timing for the roofline (apply kernel + constrained rows)
+    ts = []
+    for _ in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        op.vmult_add(dst, src64)
+        b.record(stream)
+        ts.append((a, b))
+    torch.cuda.synchronize()
+    apply_ms = float(np.mean([a.elapsed_time(b) for a, b in ts]))
+    clocks = sampler.stop()
+    if dist:
+        tt = torch.tensor([t_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    value = world * n_dofs * args.steps / (t_ms * 1e-3) / 1e9
+
+    # per-variant rates (same mesh / inputs)
+    variants = {}
+    peak, peak_kind = measured_peak()
+    for variant in () if args.no_variants else ("tensor4", "tensor2", "scalar"):
+        for prec in ("fp64", "fp32"):
+            if variant == "tensor4" and prec == "fp64":
+                v_op, s_in = op, src64
+            else:
+                v_op = make(variant, prec)
+                s_in = src64 if prec == "fp64" else src32
+                lib.lsmf_operator_set_stream(v_op.h, lsmf.vp(stream.cuda_stream))
+            d_out = torch.empty_like(s_in)
+            for _ in range(2):
+                v_op.vmult(d_out, s_in)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            reps = 5
+            a.record(stream)
+            for _ in range(reps):
+                v_op.vmult(d_out, s_in)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(b) / reps
+            by = alg_bytes(variant, 8 if prec == "fp64" else 4, n_nodes, n_qp, n_cells)
+            variants["%s_%s" % (variant, prec)] = {
+                "gdofs": round(n_dofs / (ms * 1e-3) / 1e9, 3), "ms": round(ms, 4),
+                "alg_GBps": round(by / (ms * 1e-3) / 1e9, 1), "frac_hbm": round(by / (ms * 1e-3) / 1e9 / peak, 3)}
+            if v_op is not op:
+                del v_op
+
+    # end to end through the public API with host buffers
+    src_pin = torch.tensor(src_h).pin_memory()
+    dst_pin = torch.empty(n_dofs, dtype=torch.float64).pin_memory()
+    d_src = torch.empty_like(src64)
+    for _ in range(2):
+        d_src.copy_(src_pin, non_blocking=True)
+        op.vmult(dst, d_src)
+        dst_pin.copy_(dst, non_blocking=True)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(args.steps):
+        d_src.copy_(src_pin, non_blocking=True)
+        op.vmult(dst, d_src)
+        dst_pin.copy_(dst, non_blocking=True)
+    b.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = a.elapsed_time(b) / args.steps
+    if dist:
+        tt = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e = {"value": world * n_dofs / (e2e_ms * 1e-3) / 1e9, "unit": "GDoF/s",
+           "h2d_bytes_per_step": n_dofs * 8, "d2h_bytes_per_step": n_dofs * 8}
+
+    alg = alg_bytes("tensor4", 8, n_nodes, n_qp, n_cells)
+    achieved = alg / (apply_ms * 1e-3) / 1e9
+    traffic = read_traffic()
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "peak_kind": peak_kind, "alg_bytes_per_launch": alg,
+                "kernel": "apply_kernel<2,3,double,tensor4>"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        rate, t, _ = cpu_vmult_rate(args.cells, "tensor4", False, 5)
+        cpu = {"value": rate, "unit": "GDoF/s", "cores": threads, "kind": "port",
+               "sample": "5 vmults (median) of the full %d^3 Q2 tensor4 FP64 workload, OpenMP" % args.cells}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 4), "unit": "GDoF/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_ms / args.steps, 4),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded mu field, smooth displacement, random source)",
+                "config": {"workload": "tangent vmult, tensor4 caching, FP64, %d^3-cell Q2 unit cube" % args.cells,
+                           "n_dofs": n_dofs, "n_cells": n_cells, "degree": DEGREE,
+                           "parallelism": "replicas" if world > 1 else "single GPU",
+                           "l2": "inputs larger than L2 (2.9 GB cache tables), no flush"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": 2 * args.steps, "clocks": clocks, "variants": variants}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="lsmf", choices=["lsmf", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-variants", action="store_true", help="skip the per-variant table")
+    ap.add_argument("--cells", type=int, default=N_CELLS_1D, help="cells per direction (64 = the benchmark)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_lsmf(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())
