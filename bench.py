@@ -323,7 +323,7 @@ def run_lsmf(args):
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "peak_kind": peak_kind, "alg_bytes_per_launch": alg,
-                "kernel": "apply_kernel<2,3,double,tensor4>"}
+                "kernel": "apply_fast_kernel<2,3,double,tensor4,1 stage>"}
 
     cpu = None
     if rank == 0 and not args.no_cpu:

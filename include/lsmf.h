@@ -125,6 +125,19 @@ lsmf_status lsmf_operator_precondition_jacobi(lsmf_op *op, void *d_dst, const vo
 /* m(), n(), memory_consumption() (mf_nh_operator.h:300-392) */
 int lsmf_operator_m(const lsmf_op *op);
 size_t lsmf_operator_memory_consumption(const lsmf_op *op);
+/* execution options (no reference counterpart; defaults are the fast path):
+ * LSMF_OPT_BULK_PIPELINE: depth 1..3 of the shared-memory ring through which
+ *   each warp streams its cell records with bulk copies; 0 = plain coalesced
+ *   loads; -1 (default) = per-variant choice (tensor4: 1, others: 0).  The
+ *   depth is reduced when the ring would not fit in shared memory.
+ * LSMF_OPT_BASIC_KERNEL: 1 = the basic vmult kernel (per-warp shared-memory
+ *   sweeps, plain loads); the stage mask of vmult always uses it.
+ * LSMF_OPT_MAX_WARPS: cap on warps per block of the vmult kernel (1..8;
+ *   0 = default: 8 for tensor2, 4 otherwise).
+ * A bounded device wait that runs out in the pipelined kernel is reported
+ * as LSMF_ERR_TIMEOUT by the next synchronising call on the operator. */
+enum { LSMF_OPT_BULK_PIPELINE = 1, LSMF_OPT_BASIC_KERNEL = 2, LSMF_OPT_MAX_WARPS = 3 };
+lsmf_status lsmf_operator_set_option(lsmf_op *op, int option, int value);
 /* the CUDA stream every operator call is ordered on (cudaStream_t) */
 lsmf_status lsmf_operator_set_stream(lsmf_op *op, void *stream);
 /* copy a cache table to the host for checking: which = 0 scalar / c1,

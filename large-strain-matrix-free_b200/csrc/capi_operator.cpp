@@ -123,7 +123,7 @@ lsmf_status lsmf_operator_create(lsmf_mesh *m, int level, lsmf_caching caching, 
   if (!op) return LSMF_ERR_ALLOC;
   op->mesh = m; op->level = level; op->caching = caching; op->formulation = formulation;
   op->precision = precision;
-  op->ncomp = table_components(caching, formulation);
+  op->ncomp = table_components(caching, formulation, precision);
   const Level &L = op->L();
   lsmf_status s;
   if ((s = op->d_table.alloc((size_t)L.n_cells * op->ncomp * L.nq() * op->elem())) != LSMF_OK ||
@@ -152,6 +152,23 @@ lsmf_status lsmf_operator_set_material(lsmf_op *op, const double *mu, double nu)
   LSMF_TRY(op->d_mu.upload(op->mu_host.data(), n));
   op->cached = false;
   return LSMF_OK;
+}
+
+lsmf_status lsmf_operator_set_option(lsmf_op *op, int option, int value) {
+  if (!op) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  if (option == LSMF_OPT_BULK_PIPELINE) {
+    if (value < -1 || value > 3) { set_error("pipeline depth must be -1 (auto) or 0..3"); return LSMF_ERR_INVALID_ARG; }
+    op->stages = value;
+    return LSMF_OK;
+  }
+  if (option == LSMF_OPT_BASIC_KERNEL) { op->basic = value != 0; return LSMF_OK; }
+  if (option == LSMF_OPT_MAX_WARPS) {
+    if (value < 0 || value > 8) { set_error("warps per block must be 0 (auto) or 1..8"); return LSMF_ERR_INVALID_ARG; }
+    op->max_warps = value;
+    return LSMF_OK;
+  }
+  set_error("unknown option");
+  return LSMF_ERR_INVALID_ARG;
 }
 
 lsmf_status lsmf_operator_set_stream(lsmf_op *op, void *stream) {

@@ -27,6 +27,207 @@ struct Tab {
   double N[Q][P + 1], D[Q][P + 1], w[Q];
 };
 
+// 1D tables in the arithmetic type, passed by value as a kernel parameter:
+// with compile-time indices every entry is a constant-bank operand of the
+// FMA, so the sweeps below load no shape values from memory.
+template <int P, int Q, typename T>
+struct TabT {
+  T N[Q][P + 1], D[Q][P + 1];
+};
+
+// Sum factorisation with one 1D line per lane ("row" sweeps).  Each sweep
+// maps lane -> row of the tensor it produces and unrolls the 1D contraction
+// completely; shared memory only carries the transposes between sweeps.
+//   eval:      src rows (c,k,j) in registers -> A (x) -> B (y) -> G (z) ->
+//              per-point gradient registers
+//   integrate: per-point H -> Z (z) -> Y (y) -> per-row nodal values (x)
+// Slab layout (elements of T): [9*NQ points][2*NA][3*NB].
+template <int P, int Q, typename T>
+struct SFR {
+  static constexpr int N1 = P + 1, NN = N1 * N1 * N1, NQ = Q * Q * Q;
+  static constexpr int QPL = (NQ + 31) / 32;
+  static constexpr int XR = 3 * N1 * N1;      // x rows (c,k,j)
+  static constexpr int YR = 3 * N1 * Q;       // y rows (c,k,qx)
+  static constexpr int ZR = 3 * Q * Q;        // z rows (c,qy,qx)
+  static constexpr int RPL = (XR + 31) / 32;  // x rows per lane
+  static constexpr int NA = 3 * N1 * N1 * Q;
+  static constexpr int NB = 3 * N1 * Q * Q;
+  static constexpr int SZP = 9 * NQ;
+  static constexpr int SZ = SZP + 2 * NA + 3 * NB;
+
+  // v[r][i]: value of component c at node (i, j, k) for x row r = lane + 32 r
+  static __device__ __forceinline__ void eval(const TabT<P, Q, T> &t, const T v[RPL][N1], T *slab, int lane,
+                                              T G[QPL][3][3]) {
+    T *Pt = slab, *A = slab + SZP, *B = A + 2 * NA;
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int row = lane + 32 * r;
+      if (row < XR) {
+#pragma unroll
+        for (int qx = 0; qx < Q; ++qx) {
+          T s0 = 0, s1 = 0;
+#pragma unroll
+          for (int i = 0; i < N1; ++i) {
+            s0 += t.N[qx][i] * v[r][i];
+            s1 += t.D[qx][i] * v[r][i];
+          }
+          A[row * Q + qx] = s0;
+          A[NA + row * Q + qx] = s1;
+        }
+      }
+    }
+    __syncwarp();
+    for (int row = lane; row < YR; row += 32) {
+      const int qx = row % Q, ck = row / Q;  // ck = c*N1 + k
+      T a0[N1], a1[N1];
+#pragma unroll
+      for (int j = 0; j < N1; ++j) {
+        a0[j] = A[(ck * N1 + j) * Q + qx];
+        a1[j] = A[NA + (ck * N1 + j) * Q + qx];
+      }
+#pragma unroll
+      for (int qy = 0; qy < Q; ++qy) {
+        T s00 = 0, s01 = 0, s10 = 0;
+#pragma unroll
+        for (int j = 0; j < N1; ++j) {
+          s00 += t.N[qy][j] * a0[j];
+          s01 += t.D[qy][j] * a0[j];
+          s10 += t.N[qy][j] * a1[j];
+        }
+        const int b = (ck * Q + qy) * Q + qx;
+        B[b] = s00;
+        B[NB + b] = s01;
+        B[2 * NB + b] = s10;
+      }
+    }
+    __syncwarp();
+    for (int row = lane; row < ZR; row += 32) {
+      const int qyx = row % (Q * Q), c = row / (Q * Q);
+      T b00[N1], b01[N1], b10[N1];
+#pragma unroll
+      for (int k = 0; k < N1; ++k) {
+        const int b = (c * N1 + k) * Q * Q + qyx;
+        b00[k] = B[b];
+        b01[k] = B[NB + b];
+        b10[k] = B[2 * NB + b];
+      }
+#pragma unroll
+      for (int qz = 0; qz < Q; ++qz) {
+        T gx = 0, gy = 0, gz = 0;
+#pragma unroll
+        for (int k = 0; k < N1; ++k) {
+          gx += t.N[qz][k] * b10[k];
+          gy += t.N[qz][k] * b01[k];
+          gz += t.D[qz][k] * b00[k];
+        }
+        const int q = qz * Q * Q + qyx;
+        Pt[(c * 3 + 0) * NQ + q] = gx;
+        Pt[(c * 3 + 1) * NQ + q] = gy;
+        Pt[(c * 3 + 2) * NQ + q] = gz;
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int l = 0; l < QPL; ++l) {
+      const int q = lane + 32 * l;
+      if (q < NQ) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int e = 0; e < 3; ++e) G[l][c][e] = Pt[(c * 3 + e) * NQ + q];
+      }
+    }
+    __syncwarp();
+  }
+
+  // per-point H -> out[r][i] for x row r (component c, node (i, j, k))
+  static __device__ __forceinline__ void integrate(const TabT<P, Q, T> &t, const T H[QPL][3][3], T *slab, int lane,
+                                                   T out[RPL][N1]) {
+    T *Pt = slab, *Y = slab + SZP, *Z = Y + 2 * NA;
+#pragma unroll
+    for (int l = 0; l < QPL; ++l) {
+      const int q = lane + 32 * l;
+      if (q < NQ) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int e = 0; e < 3; ++e) Pt[(c * 3 + e) * NQ + q] = H[l][c][e];
+      }
+    }
+    __syncwarp();
+    for (int row = lane; row < ZR; row += 32) {
+      const int qyx = row % (Q * Q), c = row / (Q * Q);
+      T hx[Q], hy[Q], hz[Q];
+#pragma unroll
+      for (int qz = 0; qz < Q; ++qz) {
+        const int q = qz * Q * Q + qyx;
+        hx[qz] = Pt[(c * 3 + 0) * NQ + q];
+        hy[qz] = Pt[(c * 3 + 1) * NQ + q];
+        hz[qz] = Pt[(c * 3 + 2) * NQ + q];
+      }
+#pragma unroll
+      for (int k = 0; k < N1; ++k) {
+        T sx = 0, sy = 0, sz = 0;
+#pragma unroll
+        for (int qz = 0; qz < Q; ++qz) {
+          sx += t.N[qz][k] * hx[qz];
+          sy += t.N[qz][k] * hy[qz];
+          sz += t.D[qz][k] * hz[qz];
+        }
+        const int z = (c * N1 + k) * Q * Q + qyx;
+        Z[z] = sx;
+        Z[NB + z] = sy;
+        Z[2 * NB + z] = sz;
+      }
+    }
+    __syncwarp();
+    for (int row = lane; row < YR; row += 32) {
+      const int qx = row % Q, ck = row / Q;
+      T zx[Q], zy[Q], zz[Q];
+#pragma unroll
+      for (int qy = 0; qy < Q; ++qy) {
+        const int z = (ck * Q + qy) * Q + qx;
+        zx[qy] = Z[z];
+        zy[qy] = Z[NB + z];
+        zz[qy] = Z[2 * NB + z];
+      }
+#pragma unroll
+      for (int j = 0; j < N1; ++j) {
+        T sx = 0, so = 0;
+#pragma unroll
+        for (int qy = 0; qy < Q; ++qy) {
+          sx += t.N[qy][j] * zx[qy];
+          so += t.D[qy][j] * zy[qy] + t.N[qy][j] * zz[qy];
+        }
+        const int y = (ck * N1 + j) * Q + qx;
+        Y[y] = sx;
+        Y[NA + y] = so;
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int row = lane + 32 * r;
+      if (row < XR) {
+        T yx[Q], yo[Q];
+#pragma unroll
+        for (int qx = 0; qx < Q; ++qx) {
+          yx[qx] = Y[row * Q + qx];
+          yo[qx] = Y[NA + row * Q + qx];
+        }
+#pragma unroll
+        for (int i = 0; i < N1; ++i) {
+          T s = 0;
+#pragma unroll
+          for (int qx = 0; qx < Q; ++qx) s += t.D[qx][i] * yx[qx] + t.N[qx][i] * yo[qx];
+          out[r][i] = s;
+        }
+      }
+    }
+    __syncwarp();
+  }
+};
+
 template <int P, int Q, typename T>
 struct SF {
   static constexpr int N1 = P + 1, NN = N1 * N1 * N1, NQ = Q * Q * Q;

@@ -69,6 +69,56 @@ __device__ __forceinline__ void gather(const int *__restrict__ cn, const TS *__r
 template <typename T>
 __device__ __forceinline__ void atomic_add(T *a, T v) { atomicAdd(a, v); }
 
+// ------------------------------------------------ bulk-copy (TMA) helpers
+// One-dimensional cp.async.bulk global -> shared with mbarrier completion
+// (no tensor map, no multicast): each cell record is one contiguous,
+// 16-byte aligned block of ncomp * Q^3 values.
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ uint64_t evict_first_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar, uint64_t pol) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: try_wait suspends for a hardware time slice per call, so
+// 2^22 calls are seconds; a wait that runs out reports failure instead of
+// spinning forever
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  for (int i = 0; i < (1 << 22); ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+constexpr int FLAG_DETF = 1, FLAG_TIMEOUT = 2;
+
 // ------------------------------------------------------------ cache kernel
 template <int P, int Q, typename T, int VAR>
 __global__ void __launch_bounds__(256) cache_kernel(KArgs<T> a, Tab<P, Q> tab) {
@@ -261,6 +311,185 @@ __global__ void __launch_bounds__(256) apply_kernel(KArgs<T> a, Tab<P, Q> tab) {
   }
 }
 
+
+// --------------------------------------------- apply kernel, fast path
+// The production vmult cell loop.  One warp per cell; row-per-lane sum
+// factorisation (SFR) with the 1D matrices as constant operands; the
+// gather of the next cell (node ids, src, and u for the scalar variants) is
+// prefetched into registers while the current cell is computed; with
+// STAGES == 2 each warp streams its cell records through a two-stage
+// shared-memory ring filled by cp.async.bulk (evict-first in L2), with
+// STAGES == 0 the record is read with plain coalesced loads.
+template <int P, int Q, typename T, int VAR, int STAGES>
+__global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, T> tab) {
+  using S = SFR<P, Q, T>;
+  constexpr int N1 = P + 1, NN = S::NN, NQ = S::NQ, QPL = S::QPL, RPL = S::RPL, XR = S::XR;
+  constexpr bool SCALAR = (VAR == VAR_SCALAR_F0 || VAR == VAR_SCALAR_F1);
+  const int WPB = blockDim.x >> 5;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int rec_elems = a.ncomp * NQ;
+  const uint32_t rec_bytes = (uint32_t)(rec_elems * sizeof(T));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t warp_bytes = ((STAGES * (size_t)rec_bytes + 8 * (STAGES > 0 ? STAGES : 1) + S::SZ * sizeof(T) + 127) / 128) * 128;
+  unsigned char *wbase = smem + warp * warp_bytes;
+  constexpr int NS = STAGES > 0 ? STAGES : 1;
+  T *stage[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) stage[s] = (T *)(wbase + s * rec_bytes);
+  uint64_t *bar = (uint64_t *)(wbase + STAGES * rec_bytes);
+  T *slab = (T *)(wbase + STAGES * rec_bytes + 8 * NS);
+  const int gw = blockIdx.x * WPB + warp, nw = gridDim.x * WPB;
+  uint64_t pol = 0;
+  if (STAGES > 0) {
+    pol = evict_first_policy();
+    if (lane == 0) {
+#pragma unroll
+      for (int s = 0; s < NS; ++s) mbar_init(&bar[s], 1);
+      mbar_init_fence();
+    }
+    __syncwarp();
+    if (lane == 0) {
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const int c = gw + s * nw;
+        if (c < a.n_cells) {
+          mbar_expect_tx(&bar[s], rec_bytes);
+          bulk_g2s(stage[s], a.table + (size_t)c * rec_elems, rec_bytes, &bar[s], pol);
+        }
+      }
+    }
+  }
+  // gather registers of the x rows (c, k, j) owned by this lane
+  int pk[RPL][N1];
+  T pv[RPL][N1], pu[RPL][N1];
+  auto prefetch = [&](int c) {
+    const int *cn = a.cell_nodes + (size_t)c * NN;
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int row = lane + 32 * r;
+      if (row < XR) {
+        const int comp = row / (N1 * N1), kj = row % (N1 * N1);
+#pragma unroll
+        for (int i = 0; i < N1; ++i) {
+          const int packed = __ldg(cn + kj * N1 + i);
+          pk[r][i] = packed;
+          const size_t dof = 3 * (size_t)(packed & NODE_MASK) + comp;
+          pv[r][i] = __ldg(a.src + dof);
+          if (SCALAR) pu[r][i] = __ldg(a.u + dof);
+        }
+      }
+    }
+  };
+  if (gw < a.n_cells) prefetch(gw);
+  int it = 0;
+  for (int cell = gw; cell < a.n_cells; cell += nw, ++it) {
+    const int s = it % NS;
+    const uint32_t parity = (it / NS) & 1;
+    int ck[RPL][N1];
+    T v[RPL][N1], vu[RPL][N1];
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int row = lane + 32 * r;
+      const int comp = row < XR ? row / (N1 * N1) : 0;
+      if (row >= XR) {
+#pragma unroll
+        for (int i = 0; i < N1; ++i) { ck[r][i] = 0; v[r][i] = T(0); vu[r][i] = T(0); }
+        continue;
+      }
+#pragma unroll
+      for (int i = 0; i < N1; ++i) {
+        ck[r][i] = pk[r][i];
+        // read_dof_values(src): constrained entries read as zero
+        v[r][i] = ((pk[r][i] >> (NODE_BITS + comp)) & 1) ? T(0) : pv[r][i];
+        if (SCALAR) vu[r][i] = pu[r][i];  // read_dof_values_plain(u)
+      }
+    }
+    if (cell + nw < a.n_cells) prefetch(cell + nw);
+    T G[QPL][3][3], GU[QPL][3][3];
+    if (SCALAR) S::eval(tab, vu, slab, lane, GU);
+    S::eval(tab, v, slab, lane, G);
+    const T *rec;
+    if (STAGES > 0) {
+      if (!mbar_wait_bounded(&bar[s], parity)) {
+        if (lane == 0) atomicOr(a.flag, FLAG_TIMEOUT);
+        // let the copies still in flight land before the block exits
+        for (int k = 1; k < NS; ++k)
+          if (cell + k * nw < a.n_cells) mbar_wait_bounded(&bar[(it + k) % NS], ((it + k) / NS) & 1);
+        return;
+      }
+      rec = stage[s];
+    } else {
+      rec = a.table + (size_t)cell * rec_elems;
+    }
+    T mu = 0, lambda = 0, kappa = 0;
+    if (SCALAR) material<T>(a.mu[cell], a.nu, mu, lambda, kappa);
+    T H[QPL][3][3];
+#pragma unroll
+    for (int l = 0; l < QPL; ++l) {
+      const int q = lane + 32 * l;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int e = 0; e < 3; ++e) H[l][c][e] = T(0);
+      if (q >= NQ) continue;
+      const T *r = rec + q;
+      T Ji[3][3];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) Ji[i / 3][i % 3] = r[(C_JINV + i) * NQ];
+      const T jxw = r[C_JXW * NQ];
+      T g[3][3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) g[c][d] = G[l][c][0] * Ji[0][d] + G[l][c][1] * Ji[1][d] + G[l][c][2] * Ji[2][d];
+      ScalarState<T> st;
+      if (SCALAR) {
+        T Jr[3][3];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) Jr[i / 3][i % 3] = r[(C_VAR + 1 + i) * NQ];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            st.F[c][d] = GU[l][c][0] * Jr[0][d] + GU[l][c][1] * Jr[1][d] + GU[l][c][2] * Jr[2][d] + (c == d ? T(1) : T(0));
+        st.det = det3(st.F);
+      }
+      T Qm[3][3];
+      physics<T, VAR, NQ>(g, r, mu, lambda, kappa, st, Qm);
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int e = 0; e < 3; ++e) H[l][c][e] = (Qm[c][0] * Ji[e][0] + Qm[c][1] * Ji[e][1] + Qm[c][2] * Ji[e][2]) * jxw;
+    }
+    if (STAGES > 0) {
+      __syncwarp();  // every lane is done reading stage[s]
+      if (lane == 0) {
+        const int next = cell + NS * nw;
+        if (next < a.n_cells) {
+          fence_proxy_async_smem();
+          mbar_expect_tx(&bar[s], rec_bytes);
+          bulk_g2s(stage[s], a.table + (size_t)next * rec_elems, rec_bytes, &bar[s], pol);
+        }
+      }
+    }
+    T out[RPL][N1];
+    S::integrate(tab, H, slab, lane, out);
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int row = lane + 32 * r;
+      if (row < XR) {
+        const int comp = row / (N1 * N1);
+#pragma unroll
+        for (int i = 0; i < N1; ++i) {
+          // distribute_local_to_global: constrained rows skipped
+          if (!((ck[r][i] >> (NODE_BITS + comp)) & 1))
+            atomic_add(a.dst + 3 * (size_t)(ck[r][i] & NODE_MASK) + comp, out[r][i]);
+        }
+      }
+    }
+  }
+}
+
 // --------------------------------------------------------- diagonal kernel
 // diag(a,c) = sum_q JxW n^T B_c n with n = grad_x N_a and
 // B_c[d][l] = Q(e_c (x) e_l)[c][d]: identical to applying the cell operator
@@ -393,6 +622,17 @@ int num_sms() {
   return g_num_sms;
 }
 
+template <int P, int Q, typename T>
+TabT<P, Q, T> make_tabt(const Basis &b) {
+  TabT<P, Q, T> t;
+  for (int k = 0; k < Q; ++k)
+    for (int i = 0; i <= P; ++i) {
+      t.N[k][i] = T(b.N[k * (P + 1) + i]);
+      t.D[k][i] = T(b.D[k * (P + 1) + i]);
+    }
+  return t;
+}
+
 template <int P, int Q>
 Tab<P, Q> make_tab(const Basis &b) {
   Tab<P, Q> t;
@@ -421,6 +661,12 @@ int grid_for(K kernel, int threads, size_t smem, int n_items_per_block_total) {
 inline int warps_for(size_t slab_bytes, int max_warps) {
   int w = max_warps;
   while (w > 1 && slab_bytes * w > 200 * 1024) w >>= 1;
+  return w;
+}
+// largest warp count (<= max_warps) whose slabs fit in budget bytes
+inline int warps_for_budget(size_t warp_bytes, int max_warps, size_t budget) {
+  int w = max_warps;
+  while (w > 0 && warp_bytes * w > budget) --w;
   return w;
 }
 
@@ -476,7 +722,38 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask) {
   const size_t smem = sizeof(T) * (S::TAB + w * S::SZ);
   const bool full = (mask & (LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD)) ==
                     (LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD);
-  if (full) {
+  using SR = SFR<P, Q, T>;
+  const size_t rec_bytes = (size_t)op->ncomp * S::NQ * sizeof(T);
+  const TabT<P, Q, T> tabt = make_tabt<P, Q, T>(op->mesh->basis);
+  auto wbytes = [&](int st) { return ((st * rec_bytes + 8 * (st > 0 ? st : 1) + SR::SZ * sizeof(T) + 127) / 128) * 128; };
+  // defaults measured on B200 at 64^3 Q2 (ring depth, warps per block):
+  // tensor4 streams 52 values per point and wants the bulk-copy ring;
+  // tensor2 and scalar are latency / FP64 bound and run best on plain loads
+  int stages = op->stages >= 0 ? op->stages : (VAR == VAR_TENSOR4 ? 1 : 0);
+  const int max_warps = op->max_warps > 0 ? op->max_warps : (VAR == VAR_TENSOR2 ? 8 : 4);
+  if (rec_bytes % 16 != 0) stages = 0;
+  // fewer stages when the ring would leave fewer than 4 warps per block
+  while (stages > 0 && warps_for_budget(wbytes(stages), 8, 220 * 1024) < 4) --stages;
+  if (full && !op->basic) {
+    // at most 8 warps per block (the kernel's launch bound is 256 threads);
+    // smaller blocks let several blocks share an SM
+    const int w = warps_for_budget(wbytes(stages), max_warps < 8 ? max_warps : 8, 220 * 1024);
+    const size_t smem_t = w * wbytes(stages);
+    lsmf_status st = LSMF_OK;
+    auto go = [&](auto k) -> lsmf_status {
+      LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t));
+      const int g = grid_for(k, 32 * w, smem_t, (a.n_cells + w - 1) / w);
+      k<<<g, 32 * w, smem_t, op->stream>>>(a, tabt);
+      return LSMF_OK;
+    };
+    switch (stages) {
+      case 0: st = go(apply_fast_kernel<P, Q, T, VAR, 0>); break;
+      case 1: st = go(apply_fast_kernel<P, Q, T, VAR, 1>); break;
+      case 2: st = go(apply_fast_kernel<P, Q, T, VAR, 2>); break;
+      default: st = go(apply_fast_kernel<P, Q, T, VAR, 3>); break;
+    }
+    if (st != LSMF_OK) return st;
+  } else if (full) {
     auto k = apply_kernel<P, Q, T, VAR, true>;
     LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int g = grid_for(k, 32 * w, smem, (a.n_cells + w - 1) / w);
@@ -529,10 +806,13 @@ lsmf_status run_diag(lsmf_op *op, T *diag) {
 
 }  // namespace
 
-int table_components(int caching, int formulation) {
-  if (caching == LSMF_CACHE_TENSOR4) return variant_ncomp(VAR_TENSOR4);
-  if (caching == LSMF_CACHE_TENSOR2) return variant_ncomp(VAR_TENSOR2);
+// Components per quadrature point of the cell record.  The FP32 tensor2
+// record is padded from 18 to 20 components so that every record is a
+// multiple of 16 bytes (a requirement of the bulk-copy engine).
+int table_components(int caching, int formulation, lsmf_precision precision) {
   (void)formulation;
+  if (caching == LSMF_CACHE_TENSOR4) return variant_ncomp(VAR_TENSOR4);
+  if (caching == LSMF_CACHE_TENSOR2) return variant_ncomp(VAR_TENSOR2) + (precision == LSMF_FP32 ? 2 : 0);
   return variant_ncomp(VAR_SCALAR_F1);
 }
 

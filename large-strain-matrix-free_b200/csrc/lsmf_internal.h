@@ -137,6 +137,9 @@ struct lsmf_op {
   lsmf::DevBuf<int> d_flag;          // device error word
   const void *d_u = nullptr;         // borrowed displacement
   bool cached = false, have_diag = false;
+  int stages = -1;                   // bulk-copy (TMA) ring depth of the vmult kernel (0 = plain loads, -1 auto)
+  bool basic = false;                // use the basic (smem-sweep) vmult kernel
+  int max_warps = 0;                 // warps per block cap of the vmult kernel (<= 8, 0 auto)
   cudaStream_t stream = 0;
   size_t elem() const { return precision == LSMF_FP64 ? 8 : 4; }
   lsmf::Level &L() const { return *mesh->levels[level]; }
@@ -148,5 +151,5 @@ lsmf_status launch_cache(lsmf_op *op);
 lsmf_status launch_apply(const lsmf_op *op, void *dst, const void *src, unsigned mask, bool add);
 lsmf_status launch_diagonal(lsmf_op *op);
 lsmf_status upload_basis_tables(const Basis &b);
-int table_components(int caching, int formulation);
+int table_components(int caching, int formulation, lsmf_precision precision);
 }  // namespace lsmf

@@ -82,6 +82,7 @@ SIGNATURES = {
     "lsmf_operator_m": (ctypes.c_int, [vp]),
     "lsmf_operator_memory_consumption": (ctypes.c_size_t, [vp]),
     "lsmf_operator_set_stream": (ctypes.c_int, [vp, vp]),
+    "lsmf_operator_set_option": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
     "lsmf_operator_get_table": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.POINTER(ctypes.c_size_t)]),
     "lsmf_gmg_create": (ctypes.c_int, [vp, ctypes.POINTER(GmgDesc), ctypes.POINTER(vp)]),
     "lsmf_gmg_destroy": (None, [vp]),
@@ -253,6 +254,25 @@ class NeoHookOperator:
 
     def precondition_Jacobi(self, dst, src, omega):
         check(lib().lsmf_operator_precondition_jacobi(self.h, _dptr(dst), _dptr(src), omega))
+
+    def set_pipeline(self, stages):
+        """Ring depth of the bulk-copy (TMA) record pipeline in vmult (default
+        2; 0 = plain loads).  True/False select 2/0."""
+        if stages is True:
+            stages = 2
+        check(lib().lsmf_operator_set_option(self.h, 1, int(stages)))
+
+    def set_basic_kernel(self, enable):
+        """Use the basic vmult kernel (shared-memory sweeps, plain loads)."""
+        check(lib().lsmf_operator_set_option(self.h, 2, int(bool(enable))))
+
+    def set_max_warps(self, w):
+        check(lib().lsmf_operator_set_option(self.h, 3, int(w)))
+
+    def set_stream(self, stream):
+        """Order every call on a CUDA stream (torch.cuda.Stream or raw handle)."""
+        h = getattr(stream, "cuda_stream", stream)
+        check(lib().lsmf_operator_set_stream(self.h, vp(h)))
 
     def memory_consumption(self):
         return lib().lsmf_operator_memory_consumption(self.h)

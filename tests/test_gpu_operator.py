@@ -47,12 +47,24 @@ def _rel(a, b):
 VARIANTS = [("tensor4", 1), ("tensor2", 1), ("scalar", 1), ("scalar", 0)]
 
 
+KERNELS = ["bulk1", "bulk2", "bulk3", "plain", "basic"]
+
+
+def _select(op, kernel):
+    if kernel == "basic":
+        op.set_basic_kernel(True)
+    else:
+        op.set_pipeline({"bulk1": 1, "bulk2": 2, "bulk3": 3, "plain": 0}[kernel])
+
+
 @pytest.mark.parametrize("caching,formulation", VARIANTS)
 @pytest.mark.parametrize("p", [1, 2, 3, 4])
-def test_vmult_fp64_matches_oracle(caching, formulation, p):
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_vmult_fp64_matches_oracle(caching, formulation, p, kernel):
     gm, om, cmask, mu, u, src = _setup(p=p, coarse=(2, 2, 2) if p < 4 else (1, 2, 1), level=1 if p < 4 else 1)
     ref = _oracle_op(om, cmask, mu, u, caching, formulation)
     op = lsmf.NeoHookOperator(gm, caching, formulation, "fp64")
+    _select(op, kernel)
     op.set_material(mu, 0.3)
     du = torch.tensor(u, device="cuda")
     op.cache(du)
@@ -70,10 +82,13 @@ def test_vmult_fp64_matches_oracle(caching, formulation, p):
 
 
 @pytest.mark.parametrize("caching,formulation", VARIANTS)
-def test_vmult_fp32_matches_oracle(caching, formulation):
-    gm, om, cmask, mu, u, src = _setup(p=2)
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_vmult_fp32_matches_oracle(caching, formulation, p, kernel):
+    gm, om, cmask, mu, u, src = _setup(p=p, coarse=(2, 2, 2) if p < 4 else (1, 2, 1), level=1)
     ref = _oracle_op(om, cmask, mu, u, caching, formulation)
     op = lsmf.NeoHookOperator(gm, caching, formulation, "fp32")
+    _select(op, kernel)
     op.set_material(mu, 0.3)
     du = torch.tensor(u, device="cuda", dtype=torch.float32)
     op.cache(du)
