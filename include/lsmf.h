@@ -166,8 +166,11 @@ lsmf_status lsmf_gmg_set_material(lsmf_gmg *g, const double *mu_per_fine_cell, d
 lsmf_status lsmf_gmg_setup(lsmf_gmg *g, const double *d_u_fine);
 /* PreconditionMG::vmult: one V-cycle, dst = M^-1 src (FP64 device vectors) */
 lsmf_status lsmf_gmg_vmult(lsmf_gmg *g, double *d_dst, const double *d_src);
-/* Chebyshev data of a level: eigenvalue estimates, degree, theta, delta */
+/* Chebyshev data of a level: out6 = {eig_min, eig_max (Lanczos estimates),
+ * degree, theta, delta, eigenvalue-CG iterations} */
 lsmf_status lsmf_gmg_level_info(const lsmf_gmg *g, int level, double *out6);
+/* CUDA stream of every level operation (cudaStream_t) */
+lsmf_status lsmf_gmg_set_stream(lsmf_gmg *g, void *stream);
 
 /* ---- CG (SolverCG as driven by solve_linear_system, mf_elasticity.h:3012-3214) */
 typedef struct {
@@ -193,6 +196,8 @@ void lsmf_problem_destroy(lsmf_problem *p);
 /* per fine cell shear modulus override (host array) */
 lsmf_status lsmf_problem_set_mu(lsmf_problem *p, const double *mu_per_cell);
 lsmf_status lsmf_problem_info(const lsmf_problem *p, int *n_cells, int *n_dofs, double *volume);
+/* CUDA stream of the Newton driver and its operators (cudaStream_t) */
+lsmf_status lsmf_problem_set_stream(lsmf_problem *p, void *stream);
 /* Run all load steps (Solid::run, mf_elasticity.h:1187-1235). */
 typedef struct {
   int n_steps;

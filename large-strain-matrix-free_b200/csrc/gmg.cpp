@@ -1,0 +1,399 @@
+// Geometric multigrid preconditioner and CG solver on the device.
+//
+// Replaces the deal.II objects set up in Solid::setup_matrix_free
+// (mf_elasticity.h:2079-2238: PreconditionChebyshev smoothers, coarse
+// Chebyshev-as-solver, MGTransferMatrixFree, Multigrid, PreconditionMG) and
+// the SolverCG of Solid::solve_linear_system (mf_elasticity.h:3012-3214).
+// Every level operator is an lsmf_op of the level precision; vectors stay
+// resident on the device; the host only drives the iteration and reads one
+// scalar (the residual norm) per CG iteration.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <new>
+
+#include "solver_internal.h"
+
+namespace lsmf {
+
+double tridiag_eig(const std::vector<double> &d, const std::vector<double> &e, bool want_max) {
+  const int n = (int)d.size();
+  double lo = 1e300, hi = -1e300;
+  for (int i = 0; i < n; ++i) {
+    const double r = (i > 0 ? std::fabs(e[i - 1]) : 0) + (i < n - 1 ? std::fabs(e[i]) : 0);
+    lo = std::min(lo, d[i] - r);
+    hi = std::max(hi, d[i] + r);
+  }
+  auto count_below = [&](double x) {
+    int cnt = 0;
+    double q = 1.0;
+    for (int i = 0; i < n; ++i) {
+      const double ee = (i > 0) ? e[i - 1] * e[i - 1] : 0.0;
+      q = d[i] - x - (i > 0 ? ee / q : 0.0);
+      if (q == 0.0) q = -1e-300;
+      if (q < 0) ++cnt;
+    }
+    return cnt;
+  };
+  const int k = want_max ? n - 1 : 0;
+  double a = lo, b = hi;
+  for (int it = 0; it < 200; ++it) {
+    const double mid = 0.5 * (a + b);
+    if (count_below(mid) > k) b = mid; else a = mid;
+    if (b - a <= 1e-15 * std::max(std::fabs(a), std::fabs(b))) break;
+  }
+  return 0.5 * (a + b);
+}
+
+std::vector<double> coarsen_cell_field(const lsmf_mesh &M, int level, const std::vector<double> &fine) {
+  const Level &F = *M.levels.back();
+  const Level &L = *M.levels[level];
+  const int sh = (int)M.levels.size() - 1 - level;
+  std::vector<double> out(L.n_cells, 0.0);
+  for (int c = 0; c < L.n_cells; ++c) {
+    const int i0 = L.cell_ijk[3 * c] << sh, j0 = L.cell_ijk[3 * c + 1] << sh, k0 = L.cell_ijk[3 * c + 2] << sh;
+    double s = 0;
+    int n = 0;
+    for (int k = k0; k < k0 + (1 << sh); ++k)
+      for (int j = j0; j < j0 + (1 << sh); ++j)
+        for (int i = i0; i < i0 + (1 << sh); ++i) {
+          const int fc = F.cell_of_lattice[((size_t)k * F.nc[1] + j) * F.nc[0] + i];
+          if (fc >= 0) { s += fine[fc]; ++n; }
+        }
+    out[c] = n ? s / n : 1.0;
+  }
+  return out;
+}
+
+namespace {
+
+// CG with the inverse diagonal on a level operator (PreconditionChebyshev's
+// eigenvalue estimate): start vector (i % 11) - mean, ReductionControl with
+// absolute sqrt(eps) and relative 1e-10, extreme eigenvalues of the Lanczos
+// tridiagonal matrix built from the CG coefficients.
+template <typename T>
+lsmf_status estimate_eigenvalues(lsmf_gmg *g, int l, int max_it, double &emin, double &emax, int &its) {
+  lsmf_gmg_level &GL = g->levels[l];
+  lsmf_op *op = GL.op;
+  const size_t n = (size_t)op->L().n_dofs();
+  cudaStream_t st = g->stream;
+  T *x = (T *)g->eig_vecs.ptr, *gg = x + n, *h = gg + n, *d = h + n;
+  const T *invd = (const T *)op->d_inv_diag.ptr;
+  std::vector<T> rhs(n);
+  double mean = 0;
+  for (size_t i = 0; i < n; ++i) mean += (double)(i % 11);
+  mean /= (double)n;
+  for (size_t i = 0; i < n; ++i) rhs[i] = T(mean - (double)(i % 11));  // g = A 0 - b
+  LSMF_CUDA(cudaMemcpyAsync(gg, rhs.data(), n * sizeof(T), cudaMemcpyHostToDevice, st));
+  LSMF_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), st));
+  double *sc = g->sc.ptr, *part = g->partial.ptr;
+  const bool fp32 = sizeof(T) == 4;
+  auto dot = [&](const T *a, const T *b, double &out) -> lsmf_status {
+    LSMF_TRY(dot_async(a, b, fp32, n, part, sc, SC_TMP, st));
+    LSMF_CUDA(cudaMemcpyAsync(&out, sc + SC_TMP, sizeof(double), cudaMemcpyDeviceToHost, st));
+    LSMF_CUDA(cudaStreamSynchronize(st));
+    return LSMF_OK;
+  };
+  double res2;
+  LSMF_TRY(dot(gg, gg, res2));
+  const double res0 = std::sqrt(res2);
+  const double tol = std::max(std::sqrt((double)std::numeric_limits<T>::epsilon()), 1e-10 * res0);
+  std::vector<double> dT, oT;
+  its = 0;
+  if (res0 > tol) {
+    LSMF_TRY(jacobi_async<T>(h, invd, gg, 1.0, n, st));
+    LSMF_CUDA(cudaMemsetAsync(d, 0, n * sizeof(T), st));
+    LSMF_TRY(dir_async<T>(d, h, 0.0, n, st));  // d = -h
+    double gh;
+    LSMF_TRY(dot(gg, h, gh));
+    double beta = 0, old_alpha = 0;
+    while (true) {
+      ++its;
+      LSMF_TRY(launch_apply(op, h, d, LSMF_MASK_DEFAULT, false));
+      double dh;
+      LSMF_TRY(dot(d, h, dh));
+      const double alpha = gh / dh;
+      LSMF_TRY(axpy_async<T>(x, alpha, d, n, st));
+      LSMF_TRY(axpy_async<T>(gg, alpha, h, n, st));
+      LSMF_TRY(dot(gg, gg, res2));
+      if (its > 1) {
+        dT.push_back(1.0 / alpha + beta / old_alpha);
+        oT.push_back(std::sqrt(beta) / old_alpha);
+      } else {
+        dT.push_back(1.0 / alpha);
+      }
+      if (std::sqrt(res2) <= tol || its >= max_it) break;
+      LSMF_TRY(jacobi_async<T>(h, invd, gg, 1.0, n, st));
+      beta = gh;
+      LSMF_TRY(dot(gg, h, gh));
+      beta = gh / beta;
+      LSMF_TRY(dir_async<T>(d, h, beta, n, st));
+      old_alpha = alpha;
+    }
+  }
+  emin = emax = 1.0;
+  if (!dT.empty()) {
+    emin = tridiag_eig(dT, oT, false);
+    emax = tridiag_eig(dT, oT, true);
+  }
+  return LSMF_OK;
+}
+
+// Chebyshev data from the eigenvalue estimates (degree <= 0: "solver" mode
+// with range = requested reduction, the degree from the Chebyshev error bound)
+void chebyshev_coefficients(lsmf_cheb &c, int degree, double range) {
+  const double max_eig = 1.2 * c.eig_max;
+  const double alpha = (range > 1.0) ? max_eig / range : std::min(0.9 * max_eig, c.eig_min);
+  c.degree = degree;
+  if (degree <= 0) {
+    const double actual_range = max_eig / alpha;
+    const double sigma = (1. - std::sqrt(1. / actual_range)) / (1. + std::sqrt(1. / actual_range));
+    const double eps = range;
+    c.degree = 1 + (int)(std::log(1. / eps + std::sqrt(1. / eps / eps - 1.)) / std::log(1. / sigma));
+  }
+  c.theta = 0.5 * (max_eig + alpha);
+  c.delta = 0.5 * (max_eig - alpha);
+}
+
+// PreconditionChebyshev::vmult (zero_start) / step
+template <typename T>
+lsmf_status chebyshev_run(lsmf_gmg *g, int l, bool zero_start) {
+  lsmf_gmg_level &GL = g->levels[l];
+  lsmf_op *op = GL.op;
+  const size_t n = (size_t)op->L().n_dofs();
+  cudaStream_t st = g->stream;
+  T *x = (T *)GL.x.ptr, *xold = (T *)GL.xold.ptr, *b = (T *)GL.b.ptr, *r = (T *)GL.r.ptr;
+  const T *invd = (const T *)op->d_inv_diag.ptr;
+  const lsmf_cheb &c = GL.cheb;
+  if (zero_start) {
+    LSMF_TRY(cheb_zero_async<T>(x, b, invd, c.theta, n, st));
+  } else {
+    LSMF_TRY(launch_apply(op, r, x, LSMF_MASK_DEFAULT, false));
+    LSMF_TRY(cheb_first_async<T>(x, xold, b, r, invd, c.theta, n, st));
+  }
+  if (c.degree < 2 || std::fabs(c.delta) < 1e-40) return LSMF_OK;
+  double rhok = c.delta / c.theta;
+  const double sigma = c.theta / c.delta;
+  for (int k = 0; k < c.degree - 1; ++k) {
+    LSMF_TRY(launch_apply(op, r, x, LSMF_MASK_DEFAULT, false));
+    const double rhokp = 1. / (2. * sigma - rhok);
+    const double f1 = rhokp * rhok, f2 = 2. * rhokp / c.delta;
+    rhok = rhokp;
+    LSMF_TRY(cheb_step_async<T>(x, xold, b, r, invd, f1, f2, !(zero_start && k == 0), n, st));
+  }
+  return LSMF_OK;
+}
+
+// Multigrid::level_v_step
+template <typename T>
+lsmf_status vcycle(lsmf_gmg *g, int l) {
+  if (l == 0) return chebyshev_run<T>(g, 0, true);  // MGCoarseGridApplySmoother
+  lsmf_gmg_level &GL = g->levels[l], &GC = g->levels[l - 1];
+  cudaStream_t st = g->stream;
+  const lsmf_mesh &M = *g->mesh;
+  LSMF_TRY(chebyshev_run<T>(g, l, true));  // pre-smoothing (apply: zero start)
+  LSMF_TRY(launch_apply(GL.op, GL.r.ptr, GL.x.ptr, LSMF_MASK_DEFAULT, false));
+  LSMF_CUDA(cudaMemsetAsync(GC.b.ptr, 0, (size_t)GC.op->L().n_dofs() * sizeof(T), st));
+  LSMF_TRY(restrict_add_async<T>(*M.levels[l - 1], *M.transfer[l], (const T *)GL.b.ptr, (const T *)GL.r.ptr,
+                                 (T *)GC.b.ptr, st));
+  LSMF_TRY(vcycle<T>(g, l - 1));
+  LSMF_TRY(prolongate_add_async<T>(*M.levels[l - 1], *M.transfer[l], (const T *)GC.x.ptr, (T *)GL.x.ptr, st));
+  LSMF_TRY(chebyshev_run<T>(g, l, false));  // post-smoothing (smooth: step)
+  return LSMF_OK;
+}
+
+template <typename T>
+lsmf_status gmg_setup_impl(lsmf_gmg *g, const double *d_u) {
+  const lsmf_mesh &M = *g->mesh;
+  const int nl = (int)g->levels.size();
+  cudaStream_t st = g->stream;
+  for (auto &GL : g->levels) GL.op->stream = st;
+  // interpolate_to_mg in level precision
+  const size_t nf = (size_t)M.levels[nl - 1]->n_dofs();
+  LSMF_TRY(convert_async<T, double>((T *)g->levels[nl - 1].u.ptr, d_u, nf, st));
+  for (int l = nl - 1; l > 0; --l)
+    LSMF_TRY(interpolate_async<T>(*M.levels[l - 1], *M.levels[l], *M.transfer[l], (const T *)g->levels[l].u.ptr,
+                                  (T *)g->levels[l - 1].u.ptr, st));
+  for (int l = 0; l < nl; ++l) {
+    lsmf_gmg_level &GL = g->levels[l];
+    LSMF_TRY(lsmf_operator_cache(GL.op, GL.u.ptr));
+    LSMF_TRY(lsmf_operator_compute_diagonal(GL.op));
+    const bool coarse_solver = (l == 0 && g->desc.coarse_chebyshev);
+    const int eig_its = coarse_solver && g->desc.coarse_accurate_eig ? GL.op->L().n_dofs() : g->desc.eig_cg_iterations;
+    LSMF_TRY(estimate_eigenvalues<T>(g, l, eig_its, GL.cheb.eig_min, GL.cheb.eig_max, GL.cheb.eig_iterations));
+    if (coarse_solver) chebyshev_coefficients(GL.cheb, 0, 1e-3);
+    else chebyshev_coefficients(GL.cheb, g->desc.smoother_degree, g->desc.smoothing_range);
+  }
+  g->ready = true;
+  return LSMF_OK;
+}
+
+template <typename T>
+lsmf_status gmg_vmult_impl(lsmf_gmg *g, double *dst, const double *src) {
+  const int nl = (int)g->levels.size();
+  lsmf_gmg_level &GT = g->levels[nl - 1];
+  const size_t n = (size_t)GT.op->L().n_dofs();
+  cudaStream_t st = g->stream;
+  LSMF_TRY(convert_async<T, double>((T *)GT.b.ptr, src, n, st));  // copy_to_mg
+  LSMF_TRY(vcycle<T>(g, nl - 1));
+  LSMF_TRY(convert_async<double, T>(dst, (const T *)GT.x.ptr, n, st));  // copy_from_mg
+  return LSMF_OK;
+}
+
+}  // namespace
+}  // namespace lsmf
+
+using namespace lsmf;
+
+lsmf_gmg::~lsmf_gmg() {
+  for (auto &GL : levels) lsmf_operator_destroy(GL.op);
+}
+
+extern "C" {
+
+lsmf_status lsmf_gmg_create(lsmf_mesh *m, const lsmf_gmg_desc *desc, lsmf_gmg **out) {
+  if (!m || !desc || !out) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  *out = nullptr;
+  if (desc->smoother_degree < 1 || desc->eig_cg_iterations < 1 || !(desc->smoothing_range > 1.0)) {
+    set_error("bad Chebyshev parameters");
+    return LSMF_ERR_INVALID_ARG;
+  }
+  lsmf_gmg *g = new (std::nothrow) lsmf_gmg();
+  if (!g) return LSMF_ERR_ALLOC;
+  g->mesh = m;
+  g->desc = *desc;
+  const int nl = (int)m->levels.size();
+  g->levels.resize(nl);
+  lsmf_status s = LSMF_OK;
+  size_t nmax = 0;
+  for (int l = 0; l < nl && s == LSMF_OK; ++l) {
+    lsmf_gmg_level &GL = g->levels[l];
+    s = lsmf_operator_create(m, l, (lsmf_caching)desc->caching, desc->formulation, desc->precision, &GL.op);
+    if (s != LSMF_OK) break;
+    const size_t n = (size_t)m->levels[l]->n_dofs() * g->elem();
+    nmax = std::max(nmax, n);
+    if ((s = GL.x.alloc(n)) != LSMF_OK || (s = GL.b.alloc(n)) != LSMF_OK || (s = GL.r.alloc(n)) != LSMF_OK ||
+        (s = GL.xold.alloc(n)) != LSMF_OK || (s = GL.u.alloc(n)) != LSMF_OK)
+      break;
+  }
+  if (s == LSMF_OK) s = g->sc.alloc(SC_N);
+  if (s == LSMF_OK) s = g->partial.alloc(reduce_blocks());
+  if (s == LSMF_OK) s = g->eig_vecs.alloc(4 * nmax);
+  if (s != LSMF_OK) { delete g; return s; }
+  g->mu_fine.assign(m->levels.back()->n_cells, 1.0);
+  *out = g;
+  return LSMF_OK;
+}
+
+void lsmf_gmg_destroy(lsmf_gmg *g) { delete g; }
+
+lsmf_status lsmf_gmg_set_material(lsmf_gmg *g, const double *mu, double nu) {
+  if (!g || !mu) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  const int nf = g->mesh->levels.back()->n_cells;
+  g->mu_fine.assign(mu, mu + nf);
+  g->nu = nu;
+  for (int l = 0; l < (int)g->levels.size(); ++l) {
+    const std::vector<double> ml = coarsen_cell_field(*g->mesh, l, g->mu_fine);
+    LSMF_TRY(lsmf_operator_set_material(g->levels[l].op, ml.data(), nu));
+  }
+  g->ready = false;
+  return LSMF_OK;
+}
+
+lsmf_status lsmf_gmg_setup(lsmf_gmg *g, const double *d_u) {
+  if (!g || !d_u) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  return g->desc.precision == LSMF_FP64 ? gmg_setup_impl<double>(g, d_u) : gmg_setup_impl<float>(g, d_u);
+}
+
+lsmf_status lsmf_gmg_vmult(lsmf_gmg *g, double *dst, const double *src) {
+  if (!g || !dst || !src) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  if (!g->ready) { set_error("lsmf_gmg_setup has not been called"); return LSMF_ERR_NOT_INITIALIZED; }
+  return g->desc.precision == LSMF_FP64 ? gmg_vmult_impl<double>(g, dst, src) : gmg_vmult_impl<float>(g, dst, src);
+}
+
+lsmf_status lsmf_gmg_level_info(const lsmf_gmg *g, int level, double *out6) {
+  if (!g || !out6 || level < 0 || level >= (int)g->levels.size()) { set_error("bad arguments"); return LSMF_ERR_INVALID_ARG; }
+  const lsmf_cheb &c = g->levels[level].cheb;
+  out6[0] = c.eig_min; out6[1] = c.eig_max; out6[2] = c.degree; out6[3] = c.theta; out6[4] = c.delta;
+  out6[5] = c.eig_iterations;
+  return LSMF_OK;
+}
+
+lsmf_status lsmf_gmg_set_stream(lsmf_gmg *g, void *stream) {
+  if (!g) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  g->stream = (cudaStream_t)stream;
+  for (auto &GL : g->levels) GL.op->stream = g->stream;
+  return LSMF_OK;
+}
+
+// SolverCG (deal.II form: g = A x - b, d = -P g; convergence on ||g||)
+lsmf_status lsmf_cg_solve(lsmf_op *A, int precond, double omega, lsmf_gmg *gmg, double *x, const double *b,
+                          double tol_abs, int max_it, lsmf_solve_info *info) {
+  if (!A || !x || !b) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  if (A->precision != LSMF_FP64) { set_error("the outer CG operator must be FP64"); return LSMF_ERR_INVALID_ARG; }
+  if (!A->cached) { set_error("cache() has not been called"); return LSMF_ERR_NOT_INITIALIZED; }
+  if (precond == 1 && !A->have_diag) { set_error("Jacobi needs compute_diagonal()"); return LSMF_ERR_NOT_INITIALIZED; }
+  if (precond == 2 && (!gmg || !gmg->ready)) { set_error("GMG is not set up"); return LSMF_ERR_NOT_INITIALIZED; }
+  if (precond < 0 || precond > 2) { set_error("precond must be 0, 1 or 2"); return LSMF_ERR_INVALID_ARG; }
+  const size_t n = (size_t)A->L().n_dofs();
+  cudaStream_t st = A->stream;
+  if (gmg) lsmf_gmg_set_stream(gmg, st);
+  LSMF_TRY(A->cg_g.alloc(n));
+  LSMF_TRY(A->cg_h.alloc(n));
+  LSMF_TRY(A->cg_d.alloc(n));
+  LSMF_TRY(A->sc.alloc(SC_N));
+  LSMF_TRY(A->partial.alloc(reduce_blocks()));
+  double *g = A->cg_g.ptr, *h = A->cg_h.ptr, *d = A->cg_d.ptr, *sc = A->sc.ptr, *part = A->partial.ptr;
+  auto read = [&](int slot, double &v) -> lsmf_status {
+    LSMF_CUDA(cudaMemcpyAsync(&v, sc + slot, sizeof(double), cudaMemcpyDeviceToHost, st));
+    LSMF_CUDA(cudaStreamSynchronize(st));
+    return LSMF_OK;
+  };
+  auto prec = [&](double *dst, const double *src) -> lsmf_status {
+    if (precond == 0) {
+      LSMF_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      return LSMF_OK;
+    }
+    if (precond == 1) return jacobi_async<double>(dst, (const double *)A->d_inv_diag.ptr, src, omega, n, st);
+    return lsmf_gmg_vmult(gmg, dst, src);
+  };
+  LSMF_TRY(launch_apply(A, h, x, LSMF_MASK_DEFAULT, false));
+  LSMF_TRY(neg_residual_async<double>(g, h, b, n, st));
+  LSMF_TRY(dot_async(g, g, false, n, part, sc, SC_RES2, st));
+  double res2;
+  LSMF_TRY(read(SC_RES2, res2));
+  double res = std::sqrt(res2);
+  int it = 0;
+  bool conv = res <= tol_abs;
+  if (!conv && max_it > 0) {
+    LSMF_TRY(prec(h, g));
+    LSMF_TRY(dot_async(g, h, false, n, part, sc, SC_GH0, st));
+    LSMF_TRY(cg_dir_async(d, h, n, sc, SC_GH0, SC_GH0, true, st));
+    int k = 0;
+    while (true) {
+      ++it;
+      LSMF_TRY(launch_apply(A, h, d, LSMF_MASK_DEFAULT, false));
+      LSMF_TRY(dot_async(d, h, false, n, part, sc, SC_DH, st));
+      LSMF_TRY(cg_update_async(x, g, d, h, n, sc, SC_GH0 + (k & 1), part, st));
+      LSMF_TRY(read(SC_RES2, res2));
+      res = std::sqrt(res2);
+      if (!(res == res)) break;  // NaN: report non-convergence
+      if (res <= tol_abs) { conv = true; break; }
+      if (it >= max_it) break;
+      LSMF_TRY(prec(h, g));
+      LSMF_TRY(dot_async(g, h, false, n, part, sc, SC_GH0 + ((k + 1) & 1), st));
+      LSMF_TRY(cg_dir_async(d, h, n, sc, SC_GH0 + ((k + 1) & 1), SC_GH0 + (k & 1), false, st));
+      ++k;
+    }
+  }
+  int flag = 0;
+  LSMF_CUDA(cudaMemcpyAsync(&flag, A->d_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  LSMF_CUDA(cudaStreamSynchronize(st));
+  if (info) { info->iterations = it; info->residual = res; info->converged = conv ? 1 : 0; }
+  if (flag & 2) { set_error("a bounded device wait timed out in the vmult kernel"); return LSMF_ERR_TIMEOUT; }
+  if (!conv) { set_error("CG did not reach the tolerance"); return LSMF_ERR_CG_NOT_CONVERGED; }
+  return LSMF_OK;
+}
+
+}  // extern "C"

@@ -118,6 +118,8 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 constexpr int FLAG_DETF = 1, FLAG_TIMEOUT = 2;
+// internal stage bit: gather constrained entries instead of zeroing them
+constexpr unsigned MASK_INHOM = 1u << 8;
 
 // ------------------------------------------------------------ cache kernel
 template <int P, int Q, typename T, int VAR>
@@ -235,7 +237,7 @@ __global__ void __launch_bounds__(256) apply_kernel(KArgs<T> a, Tab<P, Q> tab) {
       if (rw) gather<NN>(cn, a.u, false, V, lane);   // read_dof_values_plain(u)
       if (sf) S::eval(sN, sD, V, A, B, lane, GU);
     }
-    if (rw) gather<NN>(cn, a.src, true, V, lane);    // read_dof_values(src)
+    if (rw) gather<NN>(cn, a.src, !(a.mask & MASK_INHOM), V, lane);  // read_dof_values(src)
     else {
       for (int i = lane; i < 3 * NN; i += 32) V[i] = T(0);
       __syncwarp();
@@ -721,7 +723,8 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask) {
   const int w = warps_for(sizeof(T) * S::SZ, 8);
   const size_t smem = sizeof(T) * (S::TAB + w * S::SZ);
   const bool full = (mask & (LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD)) ==
-                    (LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD);
+                        (LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD) &&
+                    !(mask & MASK_INHOM);
   using SR = SFR<P, Q, T>;
   const size_t rec_bytes = (size_t)op->ncomp * S::NQ * sizeof(T);
   const TabT<P, Q, T> tabt = make_tabt<P, Q, T>(op->mesh->basis);
@@ -849,6 +852,20 @@ lsmf_status launch_apply(const lsmf_op *op, void *dst, const void *src, unsigned
     LSMF_CUDA(cudaGetLastError());
   }
   return LSMF_OK;
+}
+
+// K g over the constrained columns: gather without zeroing, scatter skipping
+// constrained rows (dst zeroed first, no identity rows)
+lsmf_status launch_apply_inhomogeneous(const lsmf_op *op, void *dst, const void *g) {
+  const Level &L = op->L();
+  const int v = variant_of(op);
+  LSMF_CUDA(cudaMemsetAsync(dst, 0, (size_t)L.n_dofs() * op->elem(), op->stream));
+  const unsigned mask = LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD | MASK_INHOM;
+  if (op->precision == LSMF_FP64)
+    return LSMF_DISPATCH_PQ(L.p, L.q,
+                            LSMF_DISPATCH_VAR(v, (run_apply<P_, Q_, double, V_>(op, (double *)dst, (const double *)g, mask))));
+  return LSMF_DISPATCH_PQ(L.p, L.q,
+                          LSMF_DISPATCH_VAR(v, (run_apply<P_, Q_, float, V_>(op, (float *)dst, (const float *)g, mask))));
 }
 
 lsmf_status launch_diagonal(lsmf_op *op) {

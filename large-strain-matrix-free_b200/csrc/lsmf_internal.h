@@ -18,17 +18,17 @@ namespace lsmf {
 
 void set_error(const std::string &msg);
 
-#define LSMF_CUDA(call)                                                       \
-  do {                                                                        \
-    cudaError_t e_ = (call);                                                  \
-    if (e_ != cudaSuccess) {                                                  \
-      ::lsmf::set_error(std::string(#call) + ": " + cudaGetErrorString(e_));  \
-      return LSMF_ERR_CUDA;                                                   \
-    }                                                                         \
+#define LSMF_CUDA(...)                                                            \
+  do {                                                                            \
+    cudaError_t e_ = (__VA_ARGS__);                                               \
+    if (e_ != cudaSuccess) {                                                      \
+      ::lsmf::set_error(std::string(#__VA_ARGS__) + ": " + cudaGetErrorString(e_)); \
+      return LSMF_ERR_CUDA;                                                       \
+    }                                                                             \
   } while (0)
-#define LSMF_TRY(call)                       \
+#define LSMF_TRY(...)                        \
   do {                                       \
-    lsmf_status s_ = (call);                 \
+    lsmf_status s_ = (__VA_ARGS__);          \
     if (s_ != LSMF_OK) return s_;            \
   } while (0)
 
@@ -50,6 +50,11 @@ struct DevBuf {
   DevBuf() = default;
   DevBuf(const DevBuf &) = delete;
   DevBuf &operator=(const DevBuf &) = delete;
+  DevBuf(DevBuf &&o) noexcept : ptr(o.ptr), n(o.n) { o.ptr = nullptr; o.n = 0; }
+  DevBuf &operator=(DevBuf &&o) noexcept {
+    if (this != &o) { release(); ptr = o.ptr; n = o.n; o.ptr = nullptr; o.n = 0; }
+    return *this;
+  }
   ~DevBuf() { release(); }
   void release() {
     if (ptr) cudaFree(ptr);
@@ -141,6 +146,8 @@ struct lsmf_op {
   bool basic = false;                // use the basic (smem-sweep) vmult kernel
   int max_warps = 0;                 // warps per block cap of the vmult kernel (<= 8, 0 auto)
   cudaStream_t stream = 0;
+  // CG workspace (outer FP64 CG driven through this operator)
+  lsmf::DevBuf<double> cg_g, cg_h, cg_d, sc, partial;
   size_t elem() const { return precision == LSMF_FP64 ? 8 : 4; }
   lsmf::Level &L() const { return *mesh->levels[level]; }
 };

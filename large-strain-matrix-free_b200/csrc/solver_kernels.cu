@@ -1,0 +1,666 @@
+// sm_100a kernels of the solver around the tangent operator:
+//   deterministic dot products / norms (fixed grid, two-pass reduction)
+//   fused CG vector updates with device-resident scalars
+//   Chebyshev smoother updates
+//   level transfer (MGTransferMatrixFree semantics) and displacement
+//   interpolation onto the coarse levels
+//   FP64 residual (internal force) and the adjoint cell gradient
+#include <cuda_runtime.h>
+
+#include "cell_kernels.cuh"
+#include "lsmf_internal.h"
+#include "solver_internal.h"
+
+namespace lsmf {
+
+namespace {
+
+constexpr int RED_THREADS = 256;
+
+template <typename A, typename B>
+__global__ void dot_partial_kernel(const A *a, const B *b, size_t n, double *partial) {
+  __shared__ double sh[RED_THREADS / 32];
+  double s = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    s += (double)a[i] * (double)b[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  }
+}
+
+// sums partial[0..n) in a fixed order into sc[slot]
+__global__ void reduce_final_kernel(const double *partial, int n, double *sc, int slot) {
+  __shared__ double sh[32];
+  double s = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += partial[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) sc[slot] = s;
+  }
+}
+
+// CG: alpha = sc[gh] / sc[DH]; x += alpha d; g += alpha h; partial sums of g.g
+__global__ void cg_update_kernel(double *x, double *g, const double *d, const double *h, size_t n,
+                                 const double *sc, int gh_slot, double *partial) {
+  __shared__ double sh[RED_THREADS / 32];
+  const double alpha = sc[gh_slot] / sc[SC_DH];
+  double s = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    x[i] += alpha * d[i];
+    const double gi = g[i] + alpha * h[i];
+    g[i] = gi;
+    s += gi * gi;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  }
+}
+
+// CG direction: beta = sc[gh_new] / sc[gh_old]; d = beta d - h (beta = 0: d = -h)
+__global__ void cg_dir_kernel(double *d, const double *h, size_t n, const double *sc, int gh_new, int gh_old,
+                              int first) {
+  const double beta = first ? 0.0 : sc[gh_new] / sc[gh_old];
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    d[i] = beta * d[i] - h[i];
+}
+
+template <typename T>
+__global__ void residual_init_kernel(T *g, const T *ax, const T *b, size_t n) {
+  // g = A x - b (deal.II SolverCG's negative residual)
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    g[i] = ax[i] - b[i];
+}
+
+template <typename T>
+__global__ void scaled_mul_kernel2(T *dst, const T *a, const T *b, T s, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = s * a[i] * b[i];
+}
+
+template <typename TD, typename TS>
+__global__ void convert_kernel(TD *dst, const TS *src, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = TD(src[i]);
+}
+
+template <typename T>
+__global__ void axpy_kernel(T *y, T a, const T *x, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    y[i] += a * x[i];
+}
+
+template <typename T>
+__global__ void dir_kernel(T *d, const T *h, double beta, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    d[i] = T(beta * (double)d[i] - (double)h[i]);
+}
+
+template <typename T>
+__global__ void set_indexed_kernel(T *v, const int *idx, int n, T val) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[idx[i]] = val;
+}
+
+template <typename T>
+__global__ void copy_indexed_kernel(T *dst, const T *src, const int *idx, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[idx[i]] = src[idx[i]];
+}
+
+// ---------------------------------------------------------------- Chebyshev
+// x = D^-1 b / theta                                   (vmult, zero start)
+// x_old = x; x += D^-1 (b - r) / theta                 (step, first update)
+// x_new = x + f1 (x - x_old) + f2 D^-1 (b - r); x_old = x; x = x_new
+template <typename T>
+__global__ void cheb_zero_kernel(T *x, const T *b, const T *invd, double inv_theta, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    x[i] = T((double)invd[i] * (double)b[i] * inv_theta);
+}
+template <typename T>
+__global__ void cheb_first_kernel(T *x, T *xold, const T *b, const T *r, const T *invd, double inv_theta, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const T xi = x[i];
+    xold[i] = xi;
+    x[i] = T((double)xi + (double)invd[i] * ((double)b[i] - (double)r[i]) * inv_theta);
+  }
+}
+template <typename T>
+__global__ void cheb_step_kernel(T *x, T *xold, const T *b, const T *r, const T *invd, double f1, double f2,
+                                 int has_old, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double xi = (double)x[i];
+    const double xo = has_old ? (double)xold[i] : 0.0;
+    const double xn = xi + f1 * (xi - xo) + f2 * (double)invd[i] * ((double)b[i] - (double)r[i]);
+    xold[i] = T(xi);
+    x[i] = T(xn);
+  }
+}
+
+// ------------------------------------------------------------------ transfer
+template <int P>
+struct Prol1D {
+  double m[2 * P + 1][P + 1];
+};
+
+// one warp per coarse cell.  restriction: coarse += R (weight * (b - r))
+// on the fine level, coarse Dirichlet entries dropped (restrict_and_add).
+template <int P, typename T>
+__global__ void restrict_kernel(int n_coarse, const int *__restrict__ coarse_cn, const int *__restrict__ fine_nodes,
+                                const double *__restrict__ weight, const T *__restrict__ b, const T *__restrict__ r,
+                                T *coarse, Prol1D<P> pm) {
+  constexpr int N1 = P + 1, NF = 2 * P + 1, NFB = NF * NF * NF, NCN = N1 * N1 * N1;
+  constexpr int SZ = 3 * NFB + 3 * NF * NF * N1 + 3 * NF * N1 * N1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+  double *in = (double *)smem_raw + warp * SZ, *s1 = in + 3 * NFB, *s2 = s1 + 3 * NF * NF * N1;
+  for (int c = blockIdx.x * wpb + warp; c < n_coarse; c += gridDim.x * wpb) {
+    const int *fn = fine_nodes + (size_t)c * NFB;
+    for (int l = lane; l < NFB; l += 32) {
+      const int node = fn[l];
+      const double w = weight[node];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const size_t d = 3 * (size_t)node + k;
+        in[k * NFB + l] = w * ((double)b[d] - (r ? (double)r[d] : 0.0));
+      }
+    }
+    __syncwarp();
+    // z: s1[k][z][fy][fx] = sum_fz P[fz][z] in[k][fz][fy][fx]
+    for (int it = lane; it < 3 * N1 * NF * NF; it += 32) {
+      const int fyx = it % (NF * NF), z = (it / (NF * NF)) % N1, k = it / (NF * NF * N1);
+      double s = 0;
+#pragma unroll
+      for (int fz = 0; fz < NF; ++fz) s += pm.m[fz][z] * in[k * NFB + fz * NF * NF + fyx];
+      s1[it] = s;
+    }
+    __syncwarp();
+    // y: s2[k][z][y][fx]
+    for (int it = lane; it < 3 * N1 * N1 * NF; it += 32) {
+      const int fx = it % NF, y = (it / NF) % N1, kz = it / (NF * N1);
+      double s = 0;
+#pragma unroll
+      for (int fy = 0; fy < NF; ++fy) s += pm.m[fy][y] * s1[(kz * NF + fy) * NF + fx];
+      s2[it] = s;
+    }
+    __syncwarp();
+    // x: coarse value of node (x, y, z)
+    for (int it = lane; it < 3 * NCN; it += 32) {
+      const int a = it % NCN, k = it / NCN, x = a % N1, zy = a / N1;
+      double s = 0;
+#pragma unroll
+      for (int fx = 0; fx < NF; ++fx) s += pm.m[fx][x] * s2[zy * NF + fx + k * N1 * N1 * NF];
+      const int packed = coarse_cn[(size_t)c * NCN + a];
+      if (!((packed >> (NODE_BITS + k)) & 1)) atomicAdd(coarse + 3 * (size_t)(packed & NODE_MASK) + k, T(s));
+    }
+    __syncwarp();
+  }
+}
+
+// prolongation: fine += P coarse (coarse Dirichlet entries read as zero)
+template <int P, typename T>
+__global__ void prolongate_kernel(int n_coarse, const int *__restrict__ coarse_cn, const int *__restrict__ fine_nodes,
+                                  const double *__restrict__ weight, const T *__restrict__ coarse, T *fine, Prol1D<P> pm) {
+  constexpr int N1 = P + 1, NF = 2 * P + 1, NFB = NF * NF * NF, NCN = N1 * N1 * N1;
+  constexpr int SZ = 3 * NCN + 3 * N1 * N1 * NF + 3 * N1 * NF * NF;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+  double *v = (double *)smem_raw + warp * SZ, *s1 = v + 3 * NCN, *s2 = s1 + 3 * N1 * N1 * NF;
+  for (int c = blockIdx.x * wpb + warp; c < n_coarse; c += gridDim.x * wpb) {
+    for (int it = lane; it < 3 * NCN; it += 32) {
+      const int a = it % NCN, k = it / NCN;
+      const int packed = coarse_cn[(size_t)c * NCN + a];
+      v[it] = ((packed >> (NODE_BITS + k)) & 1) ? 0.0 : (double)coarse[3 * (size_t)(packed & NODE_MASK) + k];
+    }
+    __syncwarp();
+    // x: s1[k][z][y][fx]
+    for (int it = lane; it < 3 * N1 * N1 * NF; it += 32) {
+      const int fx = it % NF, zy = it / NF;  // zy = (k*N1 + z)*N1 + y
+      double s = 0;
+#pragma unroll
+      for (int x = 0; x < N1; ++x) s += pm.m[fx][x] * v[zy * N1 + x];
+      s1[it] = s;
+    }
+    __syncwarp();
+    // y: s2[k][z][fy][fx]
+    for (int it = lane; it < 3 * N1 * NF * NF; it += 32) {
+      const int fx = it % NF, fy = (it / NF) % NF, kz = it / (NF * NF);
+      double s = 0;
+#pragma unroll
+      for (int y = 0; y < N1; ++y) s += pm.m[fy][y] * s1[(kz * N1 + y) * NF + fx];
+      s2[it] = s;
+    }
+    __syncwarp();
+    const int *fn = fine_nodes + (size_t)c * NFB;
+    for (int it = lane; it < 3 * NFB; it += 32) {
+      const int l = it % NFB, k = it / NFB, fyx = l % (NF * NF), fz = l / (NF * NF);
+      double s = 0;
+#pragma unroll
+      for (int z = 0; z < N1; ++z) s += pm.m[fz][z] * s2[(k * N1 + z) * NF * NF + fyx];
+      const int node = fn[l];
+      atomicAdd(fine + 3 * (size_t)node + k, T(weight[node] * s));
+    }
+    __syncwarp();
+  }
+}
+
+// coarse displacement at the coarse nodes from the fine one (nested
+// Lagrange spaces: evaluation of the fine field at the coarse support points)
+template <typename T>
+__global__ void interpolate_kernel(int n_coarse_nodes, int ncn, const int *__restrict__ icell,
+                                   const double *__restrict__ iw, const int *__restrict__ fine_cn,
+                                   const T *__restrict__ fine_u, T *coarse_u) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n_coarse_nodes; i += gridDim.x * blockDim.x) {
+    const int node = i / 3, k = i % 3;
+    const int fc = icell[node];
+    const double *w = iw + (size_t)node * ncn;
+    double s = 0;
+    for (int a = 0; a < ncn; ++a) s += w[a] * (double)fine_u[3 * (size_t)(fine_cn[(size_t)fc * ncn + a] & NODE_MASK) + k];
+    coarse_u[i] = T(s);
+  }
+}
+
+// ------------------------------------------------------- residual (FP64)
+// internal force per cell, -int tau : grad_x N dV (mf_elasticity.h:2760-2843
+// rhs part), evaluated in the reference configuration:
+//   H[c][f] = -sum_d tau[c][d] (J_ref^-1 F^-1)[f][d] JxW_ref
+// MODE 0: scatter into R; MODE 1: grad[cell] = lambda . (cell vector)
+template <int P, int Q, int MODE>
+__global__ void __launch_bounds__(128) internal_force_kernel(const int *__restrict__ cell_nodes, int n_cells,
+                                                              const double *__restrict__ X, const double *__restrict__ u,
+                                                              const double *__restrict__ mu_cell, double nu, int formulation,
+                                                              double *R, const double *__restrict__ lam, double *grad,
+                                                              TabT<P, Q, double> tab, Tab<P, Q> wtab) {
+  using S = SFR<P, Q, double>;
+  constexpr int N1 = P + 1, NN = S::NN, NQ = S::NQ, QPL = S::QPL, RPL = S::RPL, XR = S::XR;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+  double *slab = (double *)smem_raw + warp * S::SZ;
+  for (int cell = blockIdx.x * wpb + warp; cell < n_cells; cell += gridDim.x * wpb) {
+    const int *cn = cell_nodes + (size_t)cell * NN;
+    int ck[RPL][N1];
+    double vx[RPL][N1], vu[RPL][N1];
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int row = lane + 32 * r;
+      const int comp = row < XR ? row / (N1 * N1) : 0, kj = row % (N1 * N1);
+#pragma unroll
+      for (int i = 0; i < N1; ++i) {
+        if (row < XR) {
+          const int packed = cn[kj * N1 + i];
+          ck[r][i] = packed;
+          const size_t dof = 3 * (size_t)(packed & NODE_MASK) + comp;
+          vx[r][i] = X[dof];
+          vu[r][i] = u[dof];
+        } else {
+          ck[r][i] = 0; vx[r][i] = 0; vu[r][i] = 0;
+        }
+      }
+    }
+    double GX[QPL][3][3], GU[QPL][3][3], H[QPL][3][3];
+    S::eval(tab, vx, slab, lane, GX);
+    S::eval(tab, vu, slab, lane, GU);
+    const double mu = mu_cell[cell];
+    const double lambda = (2.0 * mu * nu) / (1.0 - 2.0 * nu);
+    const double kappa = (2.0 * mu * (1.0 + nu)) / (3.0 * (1.0 - 2.0 * nu));
+#pragma unroll
+    for (int l = 0; l < QPL; ++l) {
+      const int q = lane + 32 * l;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int e = 0; e < 3; ++e) H[l][c][e] = 0;
+      if (q >= NQ) continue;
+      const double w = wtab.w[q % Q] * wtab.w[(q / Q) % Q] * wtab.w[q / (Q * Q)];
+      double Jr[3][3], Jri[3][3], F[3][3], Fi[3][3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int e = 0; e < 3; ++e) Jr[d][e] = GX[l][d][e];
+      const double jxw = inv3(Jr, Jri) * w;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          F[c][d] = GU[l][c][0] * Jri[0][d] + GU[l][c][1] * Jri[1][d] + GU[l][c][2] * Jri[2][d] + (c == d ? 1.0 : 0.0);
+      const double det = inv3(F, Fi);
+      double b[3][3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) b[i][j] = F[i][0] * F[j][0] + F[i][1] * F[j][1] + F[i][2] * F[j][2];
+      double tau[3][3];
+      if (formulation == 0) {
+        // material.h:119-150: tau = (J dPsi_vol/dJ - tr(tau_bar)/3) I + tau_bar
+        const double s = pow(det, -2.0 / 3.0);
+        const double dPsi = (kappa / 2.0) * (det - 1.0 / det);
+        double tr = 0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) tr += b[i][i] * s * mu;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) tau[i][j] = b[i][j] * s * mu + (i == j ? dPsi * det - tr / 3.0 : 0.0);
+      } else {
+        // material.h:151-158: tau = mu b - (mu - 2 lambda ln J) I
+        const double tmp = mu - 2.0 * lambda * log(det);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) tau[i][j] = mu * b[i][j] - (i == j ? tmp : 0.0);
+      }
+      double JF[3][3];
+#pragma unroll
+      for (int f = 0; f < 3; ++f)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) JF[f][d] = Jri[f][0] * Fi[0][d] + Jri[f][1] * Fi[1][d] + Jri[f][2] * Fi[2][d];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int f = 0; f < 3; ++f)
+          H[l][c][f] = -(tau[c][0] * JF[f][0] + tau[c][1] * JF[f][1] + tau[c][2] * JF[f][2]) * jxw;
+    }
+    double out[RPL][N1];
+    S::integrate(tab, H, slab, lane, out);
+    double acc = 0;
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int row = lane + 32 * r;
+      if (row >= XR) continue;
+      const int comp = row / (N1 * N1);
+#pragma unroll
+      for (int i = 0; i < N1; ++i) {
+        const size_t dof = 3 * (size_t)(ck[r][i] & NODE_MASK) + comp;
+        if (MODE == 0) atomicAdd(R + dof, out[r][i]);
+        else acc += lam[dof] * out[r][i];
+      }
+    }
+    if (MODE == 1) {
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+      if (lane == 0) grad[cell] = acc;
+    }
+  }
+}
+
+int g_sms = 0;
+int sms() {
+  if (!g_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sms <= 0) g_sms = 148;
+  }
+  return g_sms;
+}
+inline int vec_grid(size_t n) {
+  const size_t b = (n + 255) / 256;
+  const size_t cap = (size_t)8 * sms();
+  return (int)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+}  // namespace
+
+int reduce_blocks() { return 4 * sms(); }
+
+lsmf_status dot_async(const void *a, const void *b, bool fp32, size_t n, double *partial, double *sc, int slot,
+                      cudaStream_t st) {
+  const int g = reduce_blocks();
+  if (fp32) dot_partial_kernel<float, float><<<g, RED_THREADS, 0, st>>>((const float *)a, (const float *)b, n, partial);
+  else dot_partial_kernel<double, double><<<g, RED_THREADS, 0, st>>>((const double *)a, (const double *)b, n, partial);
+  reduce_final_kernel<<<1, 1024, 0, st>>>(partial, g, sc, slot);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+
+lsmf_status cg_update_async(double *x, double *g, const double *d, const double *h, size_t n, double *sc, int gh_slot,
+                            double *partial, cudaStream_t st) {
+  const int gr = reduce_blocks();
+  cg_update_kernel<<<gr, RED_THREADS, 0, st>>>(x, g, d, h, n, sc, gh_slot, partial);
+  reduce_final_kernel<<<1, 1024, 0, st>>>(partial, gr, sc, SC_RES2);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+
+lsmf_status cg_dir_async(double *d, const double *h, size_t n, const double *sc, int gh_new, int gh_old, bool first,
+                         cudaStream_t st) {
+  cg_dir_kernel<<<vec_grid(n), 256, 0, st>>>(d, h, n, sc, gh_new, gh_old, first ? 1 : 0);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+
+template <typename T>
+lsmf_status neg_residual_async(T *g, const T *ax, const T *b, size_t n, cudaStream_t st) {
+  residual_init_kernel<T><<<vec_grid(n), 256, 0, st>>>(g, ax, b, n);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+template lsmf_status neg_residual_async<float>(float *, const float *, const float *, size_t, cudaStream_t);
+template lsmf_status neg_residual_async<double>(double *, const double *, const double *, size_t, cudaStream_t);
+
+template <typename T>
+lsmf_status jacobi_async(T *dst, const T *invd, const T *src, double omega, size_t n, cudaStream_t st) {
+  scaled_mul_kernel2<T><<<vec_grid(n), 256, 0, st>>>(dst, invd, src, T(omega), n);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+template lsmf_status jacobi_async<float>(float *, const float *, const float *, double, size_t, cudaStream_t);
+template lsmf_status jacobi_async<double>(double *, const double *, const double *, double, size_t, cudaStream_t);
+
+template <typename TD, typename TS>
+lsmf_status convert_async(TD *dst, const TS *src, size_t n, cudaStream_t st) {
+  convert_kernel<TD, TS><<<vec_grid(n), 256, 0, st>>>(dst, src, n);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+template lsmf_status convert_async<float, double>(float *, const double *, size_t, cudaStream_t);
+template lsmf_status convert_async<double, float>(double *, const float *, size_t, cudaStream_t);
+template lsmf_status convert_async<double, double>(double *, const double *, size_t, cudaStream_t);
+template lsmf_status convert_async<float, float>(float *, const float *, size_t, cudaStream_t);
+
+template <typename T>
+lsmf_status axpy_async(T *y, double a, const T *x, size_t n, cudaStream_t st) {
+  axpy_kernel<T><<<vec_grid(n), 256, 0, st>>>(y, T(a), x, n);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+template lsmf_status axpy_async<float>(float *, double, const float *, size_t, cudaStream_t);
+template lsmf_status axpy_async<double>(double *, double, const double *, size_t, cudaStream_t);
+
+template <typename T>
+lsmf_status dir_async(T *d, const T *h, double beta, size_t n, cudaStream_t st) {
+  dir_kernel<T><<<vec_grid(n), 256, 0, st>>>(d, h, beta, n);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+template lsmf_status dir_async<float>(float *, const float *, double, size_t, cudaStream_t);
+template lsmf_status dir_async<double>(double *, const double *, double, size_t, cudaStream_t);
+
+template <typename T>
+lsmf_status set_indexed_async(T *v, const int *idx, int n, double val, cudaStream_t st) {
+  if (n <= 0) return LSMF_OK;
+  set_indexed_kernel<T><<<vec_grid(n), 256, 0, st>>>(v, idx, n, T(val));
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+template lsmf_status set_indexed_async<float>(float *, const int *, int, double, cudaStream_t);
+template lsmf_status set_indexed_async<double>(double *, const int *, int, double, cudaStream_t);
+
+template <typename T>
+lsmf_status copy_indexed_async(T *dst, const T *src, const int *idx, int n, cudaStream_t st) {
+  if (n <= 0) return LSMF_OK;
+  copy_indexed_kernel<T><<<vec_grid(n), 256, 0, st>>>(dst, src, idx, n);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+template lsmf_status copy_indexed_async<double>(double *, const double *, const int *, int, cudaStream_t);
+
+template <typename T>
+lsmf_status cheb_zero_async(T *x, const T *b, const T *invd, double theta, size_t n, cudaStream_t st) {
+  cheb_zero_kernel<T><<<vec_grid(n), 256, 0, st>>>(x, b, invd, 1.0 / theta, n);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+template <typename T>
+lsmf_status cheb_first_async(T *x, T *xold, const T *b, const T *r, const T *invd, double theta, size_t n,
+                             cudaStream_t st) {
+  cheb_first_kernel<T><<<vec_grid(n), 256, 0, st>>>(x, xold, b, r, invd, 1.0 / theta, n);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+template <typename T>
+lsmf_status cheb_step_async(T *x, T *xold, const T *b, const T *r, const T *invd, double f1, double f2, bool has_old,
+                            size_t n, cudaStream_t st) {
+  cheb_step_kernel<T><<<vec_grid(n), 256, 0, st>>>(x, xold, b, r, invd, f1, f2, has_old ? 1 : 0, n);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+template lsmf_status cheb_zero_async<float>(float *, const float *, const float *, double, size_t, cudaStream_t);
+template lsmf_status cheb_zero_async<double>(double *, const double *, const double *, double, size_t, cudaStream_t);
+template lsmf_status cheb_first_async<float>(float *, float *, const float *, const float *, const float *, double, size_t,
+                                             cudaStream_t);
+template lsmf_status cheb_first_async<double>(double *, double *, const double *, const double *, const double *, double,
+                                              size_t, cudaStream_t);
+template lsmf_status cheb_step_async<float>(float *, float *, const float *, const float *, const float *, double, double,
+                                            bool, size_t, cudaStream_t);
+template lsmf_status cheb_step_async<double>(double *, double *, const double *, const double *, const double *, double,
+                                             double, bool, size_t, cudaStream_t);
+
+template <int P>
+static Prol1D<P> make_prol(const TransferMap &T) {
+  Prol1D<P> pm;
+  for (int f = 0; f < 2 * P + 1; ++f)
+    for (int x = 0; x <= P; ++x) pm.m[f][x] = T.P1[f * (P + 1) + x];
+  return pm;
+}
+
+template <typename T, int P>
+static lsmf_status transfer_impl(bool restrict_dir, const Level &C, const TransferMap &TM, const T *b, const T *r,
+                                 T *coarse_or_fine, const T *coarse_src, cudaStream_t st) {
+  constexpr int N1 = P + 1, NF = 2 * P + 1;
+  const int wpb = 4;
+  const Prol1D<P> pm = make_prol<P>(TM);
+  if (restrict_dir) {
+    constexpr int SZ = 3 * NF * NF * NF + 3 * NF * NF * N1 + 3 * NF * N1 * N1;
+    const size_t smem = sizeof(double) * SZ * wpb;
+    auto k = restrict_kernel<P, T>;
+    LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int g = (C.n_cells + wpb - 1) / wpb;
+    if (g > 16 * sms()) g = 16 * sms();
+    k<<<g, 32 * wpb, smem, st>>>(C.n_cells, C.d_cell_nodes.ptr, TM.d_fine_nodes.ptr, TM.d_weight.ptr, b, r,
+                                  coarse_or_fine, pm);
+  } else {
+    constexpr int SZ = 3 * N1 * N1 * N1 + 3 * N1 * N1 * NF + 3 * N1 * NF * NF;
+    const size_t smem = sizeof(double) * SZ * wpb;
+    auto k = prolongate_kernel<P, T>;
+    LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int g = (C.n_cells + wpb - 1) / wpb;
+    if (g > 16 * sms()) g = 16 * sms();
+    k<<<g, 32 * wpb, smem, st>>>(C.n_cells, C.d_cell_nodes.ptr, TM.d_fine_nodes.ptr, TM.d_weight.ptr, coarse_src,
+                                  coarse_or_fine, pm);
+  }
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+
+template <typename T>
+lsmf_status restrict_add_async(const Level &C, const TransferMap &TM, const T *b, const T *r, T *coarse, cudaStream_t st) {
+  switch (C.p) {
+    case 1: return transfer_impl<T, 1>(true, C, TM, b, r, coarse, nullptr, st);
+    case 2: return transfer_impl<T, 2>(true, C, TM, b, r, coarse, nullptr, st);
+    case 3: return transfer_impl<T, 3>(true, C, TM, b, r, coarse, nullptr, st);
+    case 4: return transfer_impl<T, 4>(true, C, TM, b, r, coarse, nullptr, st);
+  }
+  return LSMF_ERR_UNSUPPORTED;
+}
+template <typename T>
+lsmf_status prolongate_add_async(const Level &C, const TransferMap &TM, const T *coarse, T *fine, cudaStream_t st) {
+  switch (C.p) {
+    case 1: return transfer_impl<T, 1>(false, C, TM, nullptr, nullptr, fine, coarse, st);
+    case 2: return transfer_impl<T, 2>(false, C, TM, nullptr, nullptr, fine, coarse, st);
+    case 3: return transfer_impl<T, 3>(false, C, TM, nullptr, nullptr, fine, coarse, st);
+    case 4: return transfer_impl<T, 4>(false, C, TM, nullptr, nullptr, fine, coarse, st);
+  }
+  return LSMF_ERR_UNSUPPORTED;
+}
+template lsmf_status restrict_add_async<float>(const Level &, const TransferMap &, const float *, const float *, float *,
+                                               cudaStream_t);
+template lsmf_status restrict_add_async<double>(const Level &, const TransferMap &, const double *, const double *,
+                                                double *, cudaStream_t);
+template lsmf_status prolongate_add_async<float>(const Level &, const TransferMap &, const float *, float *, cudaStream_t);
+template lsmf_status prolongate_add_async<double>(const Level &, const TransferMap &, const double *, double *,
+                                                  cudaStream_t);
+
+template <typename T>
+lsmf_status interpolate_async(const Level &C, const Level &F, const TransferMap &TM, const T *fine_u, T *coarse_u,
+                              cudaStream_t st) {
+  interpolate_kernel<T><<<vec_grid(3 * (size_t)C.n_nodes), 256, 0, st>>>(
+      C.n_nodes, C.ncn(), TM.d_interp_cell.ptr, TM.d_interp_w.ptr, F.d_cell_nodes.ptr, fine_u, coarse_u);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+template lsmf_status interpolate_async<float>(const Level &, const Level &, const TransferMap &, const float *, float *,
+                                              cudaStream_t);
+template lsmf_status interpolate_async<double>(const Level &, const Level &, const TransferMap &, const double *,
+                                               double *, cudaStream_t);
+
+template <int P, int Q, int MODE>
+static lsmf_status internal_force_impl(const Level &L, const Basis &B, const double *u, const double *mu, double nu,
+                                       int formulation, double *R, const double *lam, double *grad, cudaStream_t st) {
+  using S = SFR<P, Q, double>;
+  TabT<P, Q, double> t;
+  Tab<P, Q> w;
+  for (int k = 0; k < Q; ++k) {
+    for (int i = 0; i <= P; ++i) {
+      t.N[k][i] = B.N[k * (P + 1) + i];
+      t.D[k][i] = B.D[k * (P + 1) + i];
+      w.N[k][i] = t.N[k][i];
+      w.D[k][i] = t.D[k][i];
+    }
+    w.w[k] = B.qw[k];
+  }
+  const int wpb = 4;
+  const size_t smem = sizeof(double) * S::SZ * wpb;
+  auto k = internal_force_kernel<P, Q, MODE>;
+  LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int g = (L.n_cells + wpb - 1) / wpb;
+  if (g > 16 * sms()) g = 16 * sms();
+  k<<<g, 32 * wpb, smem, st>>>(L.d_cell_nodes.ptr, L.n_cells, L.d_X.ptr, u, mu, nu, formulation, R, lam, grad, t, w);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+
+// R += -f_int(u) (caller initialises R with the external load)
+lsmf_status internal_force_async(const Level &L, const Basis &B, const double *u, const double *mu, double nu,
+                                 int formulation, double *R, cudaStream_t st) {
+  switch (L.p) {
+    case 1: return internal_force_impl<1, 2, 0>(L, B, u, mu, nu, formulation, R, nullptr, nullptr, st);
+    case 2: return internal_force_impl<2, 3, 0>(L, B, u, mu, nu, formulation, R, nullptr, nullptr, st);
+    case 3: return internal_force_impl<3, 4, 0>(L, B, u, mu, nu, formulation, R, nullptr, nullptr, st);
+    case 4: return internal_force_impl<4, 5, 0>(L, B, u, mu, nu, formulation, R, nullptr, nullptr, st);
+  }
+  return LSMF_ERR_UNSUPPORTED;
+}
+// grad[c] = lambda . (-f_int of cell c)
+lsmf_status adjoint_cell_grad_async(const Level &L, const Basis &B, const double *u, const double *mu, double nu,
+                                    int formulation, const double *lam, double *grad, cudaStream_t st) {
+  switch (L.p) {
+    case 1: return internal_force_impl<1, 2, 1>(L, B, u, mu, nu, formulation, nullptr, lam, grad, st);
+    case 2: return internal_force_impl<2, 3, 1>(L, B, u, mu, nu, formulation, nullptr, lam, grad, st);
+    case 3: return internal_force_impl<3, 4, 1>(L, B, u, mu, nu, formulation, nullptr, lam, grad, st);
+    case 4: return internal_force_impl<4, 5, 1>(L, B, u, mu, nu, formulation, nullptr, lam, grad, st);
+  }
+  return LSMF_ERR_UNSUPPORTED;
+}
+
+}  // namespace lsmf

@@ -90,6 +90,7 @@ SIGNATURES = {
     "lsmf_gmg_setup": (ctypes.c_int, [vp, vp]),
     "lsmf_gmg_vmult": (ctypes.c_int, [vp, vp, vp]),
     "lsmf_gmg_level_info": (ctypes.c_int, [vp, ctypes.c_int, dp]),
+    "lsmf_gmg_set_stream": (ctypes.c_int, [vp, vp]),
     "lsmf_cg_solve": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, vp, vp, vp, ctypes.c_double,
                                      ctypes.c_int, ctypes.POINTER(SolveInfo)]),
     "lsmf_problem_create": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(vp)]),
@@ -97,6 +98,7 @@ SIGNATURES = {
     "lsmf_problem_set_mu": (ctypes.c_int, [vp, dp]),
     "lsmf_problem_info": (ctypes.c_int, [vp, ip, ip, dp]),
     "lsmf_problem_run": (ctypes.c_int, [vp, ctypes.POINTER(NewtonInfo)]),
+    "lsmf_problem_set_stream": (ctypes.c_int, [vp, vp]),
     "lsmf_problem_get_solution": (ctypes.c_int, [vp, dp]),
     "lsmf_adjoint_forward": (ctypes.c_int, [vp, dp, dp, ctypes.c_int, dp]),
     "lsmf_adjoint_backward": (ctypes.c_int, [vp, dp]),
@@ -283,6 +285,112 @@ class NeoHookOperator:
         out = np.zeros(cnt.value)
         check(lib().lsmf_operator_get_table(self.h, which, out.ctypes.data_as(dp), ctypes.byref(cnt)))
         return out
+
+
+class GMG:
+    """Geometric multigrid V-cycle (PreconditionMG of mf_elasticity.h:2079-2238):
+    level operators of the given caching / precision, Chebyshev smoothing,
+    Chebyshev coarse solver, matrix-free transfer."""
+
+    def __init__(self, mesh, caching="tensor4", formulation=1, precision="fp32", degree=5, smoothing_range=20.0,
+                 eig_cg_iterations=30, coarse_chebyshev=True, coarse_accurate_eig=True):
+        d = GmgDesc()
+        d.caching = CACHING[caching] if isinstance(caching, str) else int(caching)
+        d.formulation = formulation
+        d.precision = 1 if precision in ("fp32", "float", 1) else 0
+        d.smoother_degree, d.smoothing_range, d.eig_cg_iterations = degree, smoothing_range, eig_cg_iterations
+        d.coarse_chebyshev, d.coarse_accurate_eig = int(coarse_chebyshev), int(coarse_accurate_eig)
+        h = vp()
+        check(lib().lsmf_gmg_create(mesh.h, ctypes.byref(d), ctypes.byref(h)))
+        self.h, self.mesh = h, mesh
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().lsmf_gmg_destroy(self.h)
+            self.h = None
+
+    def set_material(self, mu_fine, nu):
+        nc, _, _ = self.mesh.info(-1)
+        mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu_fine, dtype=np.float64), (nc,)))
+        check(lib().lsmf_gmg_set_material(self.h, mu.ctypes.data_as(dp), nu))
+
+    def setup(self, u_fine):
+        self._u = u_fine
+        check(lib().lsmf_gmg_setup(self.h, _dptr(u_fine)))
+
+    def vmult(self, dst, src):
+        check(lib().lsmf_gmg_vmult(self.h, _dptr(dst), _dptr(src)))
+
+    def level_info(self, level):
+        out = np.zeros(6)
+        check(lib().lsmf_gmg_level_info(self.h, level, out.ctypes.data_as(dp)))
+        return out
+
+
+def cg_solve(op, x, b, tol, max_it, precond="gmg", gmg=None, omega=1.0):
+    """SolverCG: solve op x = b to ||b - op x|| <= tol (x holds the initial guess)."""
+    info = SolveInfo()
+    pc = {"none": 0, "jacobi": 1, "gmg": 2}[precond]
+    st = lib().lsmf_cg_solve(op.h, pc, omega, gmg.h if gmg is not None else None, _dptr(x), _dptr(b), tol, max_it,
+                             ctypes.byref(info))
+    if st not in (0, 5):
+        check(st)
+    return {"iterations": info.iterations, "residual": info.residual, "converged": bool(info.converged),
+            "status": st}
+
+
+class Problem:
+    """A reference-format .prm problem (Solid of mf_elasticity.h): mesh,
+    boundary conditions, loads, FP64 fine operator, optional GMG, and the
+    device load-stepping Newton driver."""
+
+    def __init__(self, prm_text):
+        h = vp()
+        check(lib().lsmf_problem_create(prm_text.encode(), ctypes.byref(h)))
+        self.h = h
+        nc, nd, vol = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        check(lib().lsmf_problem_info(h, ctypes.byref(nc), ctypes.byref(nd), ctypes.byref(vol)))
+        self.n_cells, self.n_dofs, self.volume = nc.value, nd.value, vol.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().lsmf_problem_destroy(self.h)
+            self.h = None
+
+    def set_mu(self, mu_per_cell):
+        mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu_per_cell, dtype=np.float64), (self.n_cells,)))
+        check(lib().lsmf_problem_set_mu(self.h, mu.ctypes.data_as(dp)))
+
+    def set_stream(self, stream):
+        check(lib().lsmf_problem_set_stream(self.h, vp(getattr(stream, "cuda_stream", stream))))
+
+    def run(self, raise_on_error=True):
+        info = NewtonInfo()
+        st = lib().lsmf_problem_run(self.h, ctypes.byref(info))
+        if raise_on_error:
+            check(st)
+        steps = [{"newton_iterations": info.newton_iterations[i], "cg_iterations": info.cg_iterations[i],
+                  "point_u": [info.point_u[i][c] for c in range(3)]} for i in range(info.n_steps)]
+        return {"status": st, "steps": steps, "time_residual": info.time_residual,
+                "time_setup": info.time_setup, "time_solve": info.time_solve}
+
+    def solution(self):
+        u = np.zeros(self.n_dofs)
+        check(lib().lsmf_problem_get_solution(self.h, u.ctypes.data_as(dp)))
+        return u
+
+    def adjoint_forward(self, log_mu, u_target, obj_id):
+        lm = np.ascontiguousarray(log_mu, dtype=np.float64)
+        ut = np.ascontiguousarray(u_target, dtype=np.float64)
+        J = ctypes.c_double()
+        check(lib().lsmf_adjoint_forward(self.h, lm.ctypes.data_as(dp), ut.ctypes.data_as(dp), obj_id,
+                                         ctypes.byref(J)))
+        return J.value
+
+    def adjoint_backward(self):
+        g = np.zeros(self.n_cells)
+        check(lib().lsmf_adjoint_backward(self.h, g.ctypes.data_as(dp)))
+        return g
 
 
 class _DevArray:

@@ -250,6 +250,51 @@ class Transfer:
         return cu
 
 
+class GMG:
+    """The oracle's V-cycle preconditioner (levels 0..n_refinements)."""
+
+    def __init__(self, geometry, coarse, n_refinements, lo, hi, scale, p, q, caching, formulation, fp32, mu_fine, nu,
+                 dirichlet, u, degree=5, smoothing_range=20.0, eig_its=30, coarse_chebyshev=True,
+                 coarse_accurate_eig=True):
+        L = lib()
+        L.orc_gmg_new.restype = ctypes.c_void_p
+        L.orc_gmg_vmult.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        L.orc_gmg_level_info.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        L.orc_gmg_free.argtypes = [ctypes.c_void_p]
+        c = np.array(coarse, dtype=np.int32)
+        lo_, hi_ = np.array(lo, dtype=np.float64), np.array(hi, dtype=np.float64)
+        mu = np.ascontiguousarray(mu_fine, dtype=np.float64)
+        ids = np.array([d[0] for d in dirichlet] or [0], dtype=np.int32)
+        masks = np.array([d[1] for d in dirichlet] or [0], dtype=np.int32)
+        uu = np.ascontiguousarray(u, dtype=np.float64)
+        self.h = L.orc_gmg_new(ctypes.c_int(geometry), _ip(c), ctypes.c_int(n_refinements), _dp(lo_), _dp(hi_),
+                               ctypes.c_double(scale), ctypes.c_int(p), ctypes.c_int(q), ctypes.c_int(CACHE[caching]),
+                               ctypes.c_int(formulation), ctypes.c_int(int(fp32)), _dp(mu), ctypes.c_double(nu),
+                               ctypes.c_int(len(dirichlet)), _ip(ids), _ip(masks), _dp(uu), ctypes.c_int(degree),
+                               ctypes.c_double(smoothing_range), ctypes.c_int(eig_its),
+                               ctypes.c_int(int(coarse_chebyshev)), ctypes.c_int(int(coarse_accurate_eig)))
+        if not self.h:
+            raise RuntimeError(L.orc_last_error().decode())
+        self.n = uu.size
+        self.n_levels = n_refinements + 1
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_gmg_free(self.h)
+            self.h = None
+
+    def vmult(self, src):
+        s = np.ascontiguousarray(src, dtype=np.float64)
+        d = np.zeros_like(s)
+        lib().orc_gmg_vmult(self.h, _dp(d), _dp(s))
+        return d
+
+    def level_info(self, l):
+        out = np.zeros(6)
+        lib().orc_gmg_level_info(self.h, l, _dp(out))
+        return out
+
+
 class NewtonParams(ctypes.Structure):
     _fields_ = ([(n, ctypes.c_double * 3) for n in ("lo", "hi")] +
                 [(n, ctypes.c_double) for n in ("scale", "mu", "nu", "end_time", "dt", "tol_f", "tol_u",

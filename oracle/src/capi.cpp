@@ -179,6 +179,65 @@ void orc_transfer_interpolate(void *hh, const double *fine_u, double *coarse_u) 
   h->t.interpolate(h->c->m, h->f->m, fine_u, coarse_u);
 }
 
+// ---------------------------------------------------------------- GMG
+struct GmgH {
+  NewtonParams prm;
+  Basis1D bas;
+  std::vector<Mesh> meshes;
+  std::vector<std::vector<uint8_t>> lmask;
+  std::vector<std::vector<double>> lmu;
+  GMG<float> gf;
+  GMG<double> gd;
+  bool fp32;
+};
+// mesh description as for orc_mesh_new (levels 0..n_refinements), Dirichlet
+// specs, fine per-cell mu, fine displacement u; Chebyshev parameters
+void *orc_gmg_new(int geom, const int *coarse, int nref, const double *lo, const double *hi, double scale, int p,
+                  int q, int caching, int formulation, int fp32, const double *mu_fine, double nu, int n_dir,
+                  const int *dir_ids, const int *dir_masks, const double *u, int degree, double range, int eig_its,
+                  int coarse_cheb, int coarse_accurate) {
+  try {
+    auto *h = new GmgH();
+    NewtonParams &P = h->prm;
+    P.mesh.geometry = geom; P.mesh.n_refinements = nref; P.mesh.scale = scale; P.mesh.p = p; P.mesh.q = q;
+    for (int k = 0; k < 3; ++k) { P.mesh.coarse[k] = coarse[k]; P.mesh.lo[k] = lo[k]; P.mesh.hi[k] = hi[k]; }
+    P.caching = caching; P.formulation = formulation; P.nu = nu;
+    P.cheb_degree = degree; P.smoothing_range = range; P.cheb_eig_its = eig_its;
+    P.coarse_chebyshev = coarse_cheb; P.coarse_accurate_eig = coarse_accurate;
+    for (int i = 0; i < n_dir; ++i) P.dirichlet.push_back({dir_ids[i], dir_masks[i]});
+    h->bas.init(p, q);
+    const int nl = nref + 1;
+    h->meshes.resize(nl);
+    for (int l = 0; l < nl; ++l) build_mesh(P.mesh, l, h->meshes[l]);
+    h->lmask.resize(nl);
+    for (int l = 0; l < nl; ++l) constrained_dofs(h->meshes[l], P.dirichlet, h->lmask[l]);
+    std::vector<double> muf(mu_fine, mu_fine + h->meshes.back().n_cells);
+    h->lmu.resize(nl);
+    for (int l = 0; l < nl; ++l) h->lmu[l] = coarsen_cell_field(h->meshes, l, muf);
+    std::vector<double> uf(u, u + h->meshes.back().n_dofs());
+    h->fp32 = fp32 != 0;
+    if (h->fp32) setup_gmg<float>(P, h->meshes, h->bas, h->lmask, h->lmu, uf, h->gf, true);
+    else setup_gmg<double>(P, h->meshes, h->bas, h->lmask, h->lmu, uf, h->gd, true);
+    return h;
+  } catch (std::exception &e) { g_err = e.what(); return nullptr; }
+}
+void orc_gmg_free(void *h) { delete (GmgH *)h; }
+void orc_gmg_vmult(void *hh, double *dst, const double *src) {
+  auto *h = (GmgH *)hh;
+  const size_t n = h->meshes.back().n_dofs();
+  std::vector<double> s(src, src + n), d(n);
+  if (h->fp32) h->gf.vmult(d, s); else h->gd.vmult(d, s);
+  std::memcpy(dst, d.data(), n * sizeof(double));
+}
+void orc_gmg_level_info(void *hh, int l, double *out6) {
+  auto *h = (GmgH *)hh;
+  auto get = [&](auto &g) {
+    const auto &c = g.levels[l].cheb;
+    out6[0] = c.eig_min; out6[1] = c.eig_max; out6[2] = c.degree; out6[3] = c.theta; out6[4] = c.delta; out6[5] = 0;
+  };
+  if (h->fp32) get(h->gf); else get(h->gd);
+}
+
 // ------------------------------------------------------------- Newton
 // Flat parameter block (doubles then ints) so that ctypes can fill it.
 struct orc_newton_params {

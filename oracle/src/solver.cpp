@@ -312,10 +312,11 @@ template <typename T>
 void Chebyshev<T>::run(std::vector<T> &x, const std::vector<T> &b, bool zero_start) const {
   const size_t n = b.size();
   std::vector<T> r(n), xold(n), tmp(n);
-  int mv = degree;
+  // vmult(): x_1 = D^-1 b / theta; step(): x_1 = x_0 + D^-1 (b - A x_0) / theta;
+  // then degree - 1 recurrence steps, each with one matrix-vector product
+  const int mv = degree - 1;
   if (zero_start) {
     for (size_t i = 0; i < n; ++i) { x[i] = T(inv_diag[i] * b[i] / theta); xold[i] = T(0); }
-    mv = degree - 1;
   } else {
     op->vmult(r.data(), x.data());
     for (size_t i = 0; i < n; ++i) {
@@ -323,7 +324,7 @@ void Chebyshev<T>::run(std::vector<T> &x, const std::vector<T> &b, bool zero_sta
       x[i] = T((double)x[i] + (double)inv_diag[i] * ((double)b[i] - (double)r[i]) / theta);
     }
   }
-  if (degree < 2 && zero_start) return;
+  if (degree < 2 || std::fabs(delta) < 1e-40) return;
   double rhok = delta / theta;
   const double sigma = theta / delta;
   for (int k = 0; k < mv; ++k) {
@@ -436,11 +437,31 @@ bool point_value(const Mesh &m, const Basis1D &b, const double *u, const double 
   return false;
 }
 
+// Per-cell values on level l from a fine per-cell field: mean over the fine
+// cells inside each level cell (the coarse-level material of a per-cell mu).
+std::vector<double> coarsen_cell_field(const std::vector<Mesh> &meshes, int l, const std::vector<double> &fine) {
+  const Mesh &F = meshes.back(), &L = meshes[l];
+  const int sh = (int)meshes.size() - 1 - l;
+  std::vector<double> out(L.n_cells, 1.0);
+  for (int c = 0; c < L.n_cells; ++c) {
+    const int i0 = L.cell_ijk[3 * c] << sh, j0 = L.cell_ijk[3 * c + 1] << sh, k0 = L.cell_ijk[3 * c + 2] << sh;
+    double s = 0; int n = 0;
+    for (int k = k0; k < k0 + (1 << sh); ++k)
+      for (int j = j0; j < j0 + (1 << sh); ++j)
+        for (int i = i0; i < i0 + (1 << sh); ++i) {
+          const int fc = F.cell_of_lattice[((size_t)k * F.nc[1] + j) * F.nc[0] + i];
+          if (fc >= 0) { s += fine[fc]; ++n; }
+        }
+    if (n) out[c] = s / n;
+  }
+  return out;
+}
+
 // --------------------------------------------------------------- Newton
 // Solid::run / solve_nonlinear_timestep / check_convergence /
 // solve_linear_system (mf_elasticity.h:1187-1235, 2245-2559, 3012-3214).
 template <typename LT>
-static void setup_gmg(const NewtonParams &prm, const std::vector<Mesh> &meshes, const Basis1D &bas,
+void setup_gmg(const NewtonParams &prm, const std::vector<Mesh> &meshes, const Basis1D &bas,
                       const std::vector<std::vector<uint8_t>> &lmask,
                       const std::vector<std::vector<double>> &lmu,
                       const std::vector<double> &u_fine, GMG<LT> &gmg, bool first) {
@@ -487,19 +508,10 @@ int newton_run(const NewtonParams &prm, NewtonResult &res) {
   res.n_cells = m.n_cells; res.n_dofs = m.n_dofs();
   res.volume = mesh_volume(m, bas);
   // per-cell shear modulus on every level (children inherit the parent's)
+  std::vector<double> mu_f = prm.mu_fine;
+  if (mu_f.empty()) mu_f.assign(m.n_cells, prm.mu);
   std::vector<std::vector<double>> lmu(nl);
-  for (int l = 0; l < nl; ++l) {
-    lmu[l].resize(meshes[l].n_cells);
-    for (int c = 0; c < meshes[l].n_cells; ++c) {
-      if (prm.mu_fine.empty()) { lmu[l][c] = prm.mu; continue; }
-      // map to a fine cell: fine index = level index << (nl-1-l)
-      const int sh = nl - 1 - l;
-      int fi = meshes[l].cell_ijk[3 * c] << sh, fj = meshes[l].cell_ijk[3 * c + 1] << sh,
-          fk = meshes[l].cell_ijk[3 * c + 2] << sh;
-      int fc = m.cell_of_lattice[((size_t)fk * m.nc[1] + fj) * m.nc[0] + fi];
-      lmu[l][c] = prm.mu_fine[fc];
-    }
-  }
+  for (int l = 0; l < nl; ++l) lmu[l] = coarsen_cell_field(meshes, l, mu_f);
   std::vector<std::vector<uint8_t>> lmask(nl);
   for (int l = 0; l < nl; ++l) constrained_dofs(meshes[l], prm.dirichlet, lmask[l]);
   const std::vector<uint8_t> &cmask = lmask[nl - 1];
@@ -595,4 +607,13 @@ int newton_run(const NewtonParams &prm, NewtonResult &res) {
   return 0;
 }
 
+}  // namespace orc
+
+namespace orc {
+template void setup_gmg<float>(const NewtonParams &, const std::vector<Mesh> &, const Basis1D &,
+                               const std::vector<std::vector<uint8_t>> &, const std::vector<std::vector<double>> &,
+                               const std::vector<double> &, GMG<float> &, bool);
+template void setup_gmg<double>(const NewtonParams &, const std::vector<Mesh> &, const Basis1D &,
+                                const std::vector<std::vector<uint8_t>> &, const std::vector<std::vector<double>> &,
+                                const std::vector<double> &, GMG<double> &, bool);
 }  // namespace orc

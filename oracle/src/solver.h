@@ -87,6 +87,11 @@ struct NewtonResult {
 };
 
 bool point_value(const Mesh &m, const Basis1D &b, const double *u, const double pt[3], double out[3]);
+std::vector<double> coarsen_cell_field(const std::vector<Mesh> &meshes, int l, const std::vector<double> &fine);
+template <typename LT>
+void setup_gmg(const NewtonParams &prm, const std::vector<Mesh> &meshes, const Basis1D &bas,
+               const std::vector<std::vector<uint8_t>> &lmask, const std::vector<std::vector<double>> &lmu,
+               const std::vector<double> &u_fine, GMG<LT> &gmg, bool first);
 int newton_run(const NewtonParams &prm, NewtonResult &res);
 
 }  // namespace orc
