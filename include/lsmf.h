@@ -192,6 +192,9 @@ lsmf_status lsmf_cg_solve(lsmf_op *fine, int precond, double omega, lsmf_gmg *gm
  * mf_elasticity.h:156-607) plus the additive keys documented in
  * INTEGRATION.md, build mesh, operators, GMG and loads. */
 lsmf_status lsmf_problem_create(const char *prm_text, lsmf_problem **out);
+/* Parse and check a .prm text without touching the device (undeclared keys,
+ * bad values and unsupported options give LSMF_ERR_PRM / _UNSUPPORTED). */
+lsmf_status lsmf_prm_validate(const char *prm_text);
 void lsmf_problem_destroy(lsmf_problem *p);
 /* per fine cell shear modulus override (host array) */
 lsmf_status lsmf_problem_set_mu(lsmf_problem *p, const double *mu_per_cell);

@@ -383,18 +383,15 @@ lsmf_problem::~lsmf_problem() {
 
 extern "C" {
 
-lsmf_status lsmf_problem_create(const char *text, lsmf_problem **out) {
-  if (!text || !out) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
-  *out = nullptr;
-  ProblemParams P;
-  LSMF_TRY(parse_prm(text, P));
+// Checks of a parsed parameter set that do not need a device (the
+// reference's AssertThrow / ParameterHandler pattern checks).
+static lsmf_status validate_params(const ProblemParams &P, int &caching) {
   if (P.dim != 3) { set_error("only Dimension = 3 is supported"); return LSMF_ERR_UNSUPPORTED; }
   if (P.solver_type != "MF_CG") { set_error("Solver type " + P.solver_type + " is not supported (MF_CG only)"); return LSMF_ERR_UNSUPPORTED; }
   if (P.precond != "jacobi" && P.precond != "gmg" && P.precond != "none") {
     set_error("Preconditioner type " + P.precond + " is not supported (jacobi | gmg | none)");
     return LSMF_ERR_UNSUPPORTED;
   }
-  int caching;
   if (P.caching == "scalar") caching = LSMF_CACHE_SCALAR;
   else if (P.caching == "tensor2") caching = LSMF_CACHE_TENSOR2;
   else if (P.caching == "tensor4") caching = LSMF_CACHE_TENSOR4;
@@ -402,15 +399,48 @@ lsmf_status lsmf_problem_create(const char *text, lsmf_problem **out) {
     set_error("MF caching " + P.caching + " is not supported");
     return LSMF_ERR_UNSUPPORTED;
   } else { set_error("Unknown caching"); return LSMF_ERR_UNKNOWN_CACHING; }
+  if (P.formulation != 0 && P.formulation != 1) { set_error("Unknown material formulation"); return LSMF_ERR_PRM; }
+  if (P.formulation == 0 && caching != LSMF_CACHE_SCALAR) {
+    set_error("formulation 0 requires scalar caching");
+    return LSMF_ERR_UNSUPPORTED;
+  }
+  if (P.degree < 1 || P.degree > 4 || P.quad_order != P.degree + 1) {
+    set_error("supported elements: Polynomial degree 1..4 with Quadrature order = degree + 1");
+    return LSMF_ERR_UNSUPPORTED;
+  }
   if (P.level_precision != "float" && P.level_precision != "double") {
     set_error("MF level precision must be float or double");
     return LSMF_ERR_PRM;
   }
+  if (P.type != "Cook" && P.type != "Box") {
+    set_error("Geometry Type " + P.type + " is not supported (Cook | Box)");
+    return LSMF_ERR_UNSUPPORTED;
+  }
+  if (!(P.nu > -1.0 && P.nu < 0.5) || !(P.mu > 0.0)) { set_error("bad material parameters"); return LSMF_ERR_PRM; }
+  if (!(P.dt > 0.0)) { set_error("Time step size must be positive"); return LSMF_ERR_PRM; }
   for (const BCExpr &d : P.dirichlet)
     if (!P.dirichlet_mask.count(d.id)) {
       set_error("Could not find component mask for ID " + std::to_string(d.id));
       return LSMF_ERR_PRM;
     }
+  return LSMF_OK;
+}
+
+lsmf_status lsmf_prm_validate(const char *text) {
+  if (!text) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  ProblemParams P;
+  LSMF_TRY(parse_prm(text, P));
+  int caching = 0;
+  return validate_params(P, caching);
+}
+
+lsmf_status lsmf_problem_create(const char *text, lsmf_problem **out) {
+  if (!text || !out) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  *out = nullptr;
+  ProblemParams P;
+  LSMF_TRY(parse_prm(text, P));
+  int caching = 0;
+  LSMF_TRY(validate_params(P, caching));
   lsmf_mesh_desc md{};
   md.degree = P.degree;
   md.n_q_points_1d = P.quad_order;
@@ -431,9 +461,6 @@ lsmf_status lsmf_problem_create(const char *text, lsmf_problem **out) {
       act = void_mask(P);
       md.coarse_active = act.data();
     }
-  } else {
-    set_error("Geometry Type " + P.type + " is not supported (Cook | Box)");
-    return LSMF_ERR_UNSUPPORTED;
   }
   lsmf_problem *pb = new (std::nothrow) lsmf_problem();
   if (!pb) return LSMF_ERR_ALLOC;

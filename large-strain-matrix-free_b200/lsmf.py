@@ -94,6 +94,7 @@ SIGNATURES = {
     "lsmf_cg_solve": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, vp, vp, vp, ctypes.c_double,
                                      ctypes.c_int, ctypes.POINTER(SolveInfo)]),
     "lsmf_problem_create": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(vp)]),
+    "lsmf_prm_validate": (ctypes.c_int, [ctypes.c_char_p]),
     "lsmf_problem_destroy": (None, [vp]),
     "lsmf_problem_set_mu": (ctypes.c_int, [vp, dp]),
     "lsmf_problem_info": (ctypes.c_int, [vp, ip, ip, dp]),
@@ -337,6 +338,12 @@ def cg_solve(op, x, b, tol, max_it, precond="gmg", gmg=None, omega=1.0):
         check(st)
     return {"iterations": info.iterations, "residual": info.residual, "converged": bool(info.converged),
             "status": st}
+
+
+def prm_validate(prm_text):
+    """Parse and check a .prm text on the host; returns (status, message)."""
+    st = lib().lsmf_prm_validate(prm_text.encode())
+    return st, (lib().lsmf_last_error().decode() if st else "")
 
 
 class Problem:
