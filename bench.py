@@ -187,6 +187,54 @@ def run_reference(args):
     return 0
 
 
+# ----------------------------------------------------- Newton step (GPU)
+def voids_prm(level_precision, cells=15, refinements=2, degree=4):
+    """Heterogeneous voids problem: unit cube with 16 seeded spherical voids
+    of radius 0.08 removed on the coarse mesh (15^3 coarse cells, 2
+    refinements: 60^3 Q2 cells, ~5 M DoFs), mu = 1, nu = 0.3, bottom face
+    clamped, top face displaced by -0.01 in z (the first of 10 load steps of
+    -0.1 in total), FP64 outer CG to 1e-8 relative residual, Chebyshev
+    smoother of the given degree on FP32 or FP64 level operators."""
+    return "\n".join([
+        "subsection Finite element system", "  set Polynomial degree = 2", "  set Quadrature order = 3", "end",
+        "subsection Geometry", "  set Dimension = 3", "  set Type = Box", "  set Box cells = %d, %d, %d" % ((cells,) * 3),
+        "  set Global refinement = %d" % refinements, "  set Void spheres = 16, 0.08, 2024", "end",
+        "subsection Material properties", "  set Shear modulus = 1", "  set Poisson's ratio = 0.3",
+        "  set Formulation = 1", "end",
+        "subsection Linear solver", "  set Solver type = MF_CG", "  set Residual = 1e-8",
+        "  set Preconditioner type = gmg", "  set MF caching = tensor4", "  set MF level precision = %s" % level_precision,
+        "  set MF Chebyshev degree = %d" % degree, "end",
+        "subsection Boundary conditions", "  set Dirichlet IDs and expressions = 4:0,0,0;5:0,0,-0.01",
+        "  set Dirichlet IDs and component mask = 4:true,true,true;5:false,false,true", "end",
+        "subsection Time", "  set End time = 0.1", "  set Time step size = 0.1", "end", ""])
+
+
+def newton_step_times(cells=15, refinements=2):
+    """Run one load step of the voids problem with FP32 and with FP64 level
+    operators; return per-form Newton-step times (device-timed residual +
+    set-up + CG) and the relative difference of the two solutions."""
+    import lsmf
+    out = {}
+    sols = {}
+    for form, prec in (("fp32_gmg", "float"), ("fp64_gmg", "double")):
+        pb = lsmf.Problem(voids_prm(prec, cells, refinements))
+        res = pb.run()
+        st = res["steps"][0]
+        its = max(1, st["newton_iterations"])
+        total = res["time_residual"] + res["time_setup"] + res["time_solve"]
+        out[form] = {"n_dofs": pb.n_dofs, "newton_iterations": st["newton_iterations"],
+                     "cg_iterations": st["cg_iterations"], "s_per_newton_step": round(total / its, 4),
+                     "residual_s": round(res["time_residual"], 4), "setup_s": round(res["time_setup"], 4),
+                     "solve_s": round(res["time_solve"], 4)}
+        sols[form] = pb.solution()
+        del pb
+    a, b = sols["fp32_gmg"], sols["fp64_gmg"]
+    out["speedup_fp32_over_fp64"] = round(out["fp64_gmg"]["s_per_newton_step"] / out["fp32_gmg"]["s_per_newton_step"], 3)
+    out["solution_rel_diff"] = float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+    out["workload"] = "voids: 60^3 Q2 cube minus 16 spheres r=0.08, tensor4, first load step, CG to 1e-8"
+    return out
+
+
 # ---------------------------------------------------------------- GPU (lsmf)
 def run_lsmf(args):
     import torch
@@ -325,6 +373,11 @@ def run_lsmf(args):
                 "peak_kind": peak_kind, "alg_bytes_per_launch": alg,
                 "kernel": "apply_fast_kernel<2,3,double,tensor4,1 stage>"}
 
+    newton = None
+    if not args.no_newton:
+        torch.cuda.synchronize()
+        newton = newton_step_times()
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -342,7 +395,8 @@ def run_lsmf(args):
                            "parallelism": "replicas" if world > 1 else "single GPU",
                            "l2": "inputs larger than L2 (2.9 GB cache tables), no flush"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": 2 * args.steps, "clocks": clocks, "variants": variants}
+                "gpu_launches": 2 * args.steps, "clocks": clocks, "variants": variants,
+                "newton_step": newton}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -358,6 +412,7 @@ def main():
     ap.add_argument("--impl", default="lsmf", choices=["lsmf", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-variants", action="store_true", help="skip the per-variant table")
+    ap.add_argument("--no-newton", action="store_true", help="skip the FP32-GMG vs FP64 Newton-step comparison")
     ap.add_argument("--cells", type=int, default=N_CELLS_1D, help="cells per direction (64 = the benchmark)")
     args = ap.parse_args()
     if args.impl == "reference":
