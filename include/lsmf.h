@@ -213,6 +213,22 @@ lsmf_status lsmf_problem_run(lsmf_problem *p, lsmf_newton_info *info);
 /* final displacement (host, n_dofs doubles) */
 lsmf_status lsmf_problem_get_solution(const lsmf_problem *p, double *host_u);
 
+/* ---- allocation-free residual norm (no counterpart in the reference) ----
+ * *d_norm = ||d_b - A d_x||_2 for a cached FP64 operator, computed without
+ * any device allocation: for callers that cannot call cudaMalloc while they
+ * run (their device memory is owned by another framework's caching
+ * allocator, or a no-allocation-after-start-up rule applies).  The scratch
+ * (A x and the reduction partials) is a static device array of
+ * LSMF_NOALLOC_MAX_DOFS + 1024 doubles (16 MiB) that every GPU loading the
+ * library keeps until exit; operators with more dofs are rejected with
+ * LSMF_ERR_INVALID_ARG.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  All calls share the array, so calls that overlap on the GPU
+ * (different streams, no ordering between them) race.  Asynchronous on the
+ * operator's stream; d_norm is a device pointer to one double. */
+#define LSMF_NOALLOC_MAX_DOFS 2097152
+lsmf_status lsmf_residual_norm_noalloc(lsmf_op *op, const double *d_x, const double *d_b, double *d_norm);
+
 /* ---- adjoint gradient (new, no reference counterpart) ----
  * forward: solve with mu = exp(log_mu) per fine cell; J = 1/2 sum over the
  * dofs of boundary id `obj_id` of (u - u_target)^2.

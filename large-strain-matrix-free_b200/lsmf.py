@@ -103,6 +103,7 @@ SIGNATURES = {
     "lsmf_problem_get_solution": (ctypes.c_int, [vp, dp]),
     "lsmf_adjoint_forward": (ctypes.c_int, [vp, dp, dp, ctypes.c_int, dp]),
     "lsmf_adjoint_backward": (ctypes.c_int, [vp, dp]),
+    "lsmf_residual_norm_noalloc": (ctypes.c_int, [vp, vp, vp, vp]),
 }
 
 
@@ -276,6 +277,11 @@ class NeoHookOperator:
         """Order every call on a CUDA stream (torch.cuda.Stream or raw handle)."""
         h = getattr(stream, "cuda_stream", stream)
         check(lib().lsmf_operator_set_stream(self.h, vp(h)))
+
+    def residual_norm_noalloc(self, x, b, out):
+        """out[0] = ||b - A x|| without any device allocation (FP64 operators
+        up to 2,097,152 dofs; the scratch is a static device array)."""
+        check(lib().lsmf_residual_norm_noalloc(self.h, _dptr(x), _dptr(b), _dptr(out)))
 
     def memory_consumption(self):
         return lib().lsmf_operator_memory_consumption(self.h)
