@@ -216,6 +216,10 @@ def newton_step_times(cells=15, refinements=2):
     import lsmf
     out = {}
     sols = {}
+    # warm-up on a small mesh so that module loading and first-launch costs
+    # are not charged to the first form
+    for prec in ("float", "double"):
+        lsmf.Problem(voids_prm(prec, 4, 1)).run()
     for form, prec in (("fp32_gmg", "float"), ("fp64_gmg", "double")):
         pb = lsmf.Problem(voids_prm(prec, cells, refinements))
         res = pb.run()
@@ -413,10 +417,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-variants", action="store_true", help="skip the per-variant table")
     ap.add_argument("--no-newton", action="store_true", help="skip the FP32-GMG vs FP64 Newton-step comparison")
+    ap.add_argument("--newton-only", action="store_true", help="only the Newton-step comparison")
+    ap.add_argument("--newton-cells", type=int, default=15, help="coarse cells per direction of the voids mesh")
+    ap.add_argument("--newton-refinements", type=int, default=2)
     ap.add_argument("--cells", type=int, default=N_CELLS_1D, help="cells per direction (64 = the benchmark)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.newton_only:
+        print(json.dumps(newton_step_times(args.newton_cells, args.newton_refinements)), flush=True)
+        return 0
     return run_lsmf(args)
 
 

@@ -105,31 +105,51 @@ lsmf_status estimate_eigenvalues(lsmf_gmg *g, int l, int max_it, double &emin, d
     LSMF_TRY(jacobi_async<T>(h, invd, gg, 1.0, n, st));
     LSMF_CUDA(cudaMemsetAsync(d, 0, n * sizeof(T), st));
     LSMF_TRY(dir_async<T>(d, h, 0.0, n, st));  // d = -h
-    double gh;
-    LSMF_TRY(dot(gg, h, gh));
-    double beta = 0, old_alpha = 0;
-    while (true) {
-      ++its;
-      LSMF_TRY(launch_apply(op, h, d, LSMF_MASK_DEFAULT, false));
-      double dh;
-      LSMF_TRY(dot(d, h, dh));
-      const double alpha = gh / dh;
-      LSMF_TRY(axpy_async<T>(x, alpha, d, n, st));
-      LSMF_TRY(axpy_async<T>(gg, alpha, h, n, st));
-      LSMF_TRY(dot(gg, gg, res2));
-      if (its > 1) {
-        dT.push_back(1.0 / alpha + beta / old_alpha);
-        oT.push_back(std::sqrt(beta) / old_alpha);
-      } else {
-        dT.push_back(1.0 / alpha);
+    LSMF_TRY(dot_async(gg, h, fp32, n, part, sc, SC_GH0, st));
+    // CG iterations run in batches of 8 with device-resident scalars; the
+    // alpha / beta / residual history is read once per batch and the Lanczos
+    // matrix is cut at the first iteration that meets the tolerance, so the
+    // estimate equals the one of an iteration checked every step
+    // one history buffer for every level (sized for the largest iteration
+    // budget, so no level re-allocates it)
+    size_t need = 0;
+    for (const auto &L : g->levels) need = std::max(need, (size_t)L.op->L().n_dofs());
+    need = 3 * (std::max(need, (size_t)g->desc.eig_cg_iterations) + 8);
+    if (g->eig_hist.n < need) LSMF_TRY(g->eig_hist.alloc(need));
+    const size_t stride = need / 3;
+    double *ha = g->eig_hist.ptr, *hb = ha + stride, *hr = hb + stride;
+    int k = 0;
+    bool done = false;
+    std::vector<double> A(8), Bt(8), Rs(8);
+    double prev_beta = 0, prev_alpha = 0;
+    while (!done && k < max_it) {
+      const int batch = std::min(8, max_it - k);
+      for (int j = 0; j < batch; ++j, ++k) {
+        const int gh = SC_GH0 + (k & 1), ghn = SC_GH0 + ((k + 1) & 1);
+        LSMF_TRY(launch_apply(op, h, d, LSMF_MASK_DEFAULT, false));
+        LSMF_TRY(dot_async(d, h, fp32, n, part, sc, SC_DH, st));
+        LSMF_TRY(eig_update_async<T>(gg, h, n, sc, gh, ha, hr, k, part, st));
+        LSMF_TRY(jacobi_async<T>(h, invd, gg, 1.0, n, st));
+        LSMF_TRY(dot_async(gg, h, fp32, n, part, sc, ghn, st));
+        LSMF_TRY(eig_dir_async<T>(d, h, n, sc, ghn, gh, hb, k, st));
       }
-      if (std::sqrt(res2) <= tol || its >= max_it) break;
-      LSMF_TRY(jacobi_async<T>(h, invd, gg, 1.0, n, st));
-      beta = gh;
-      LSMF_TRY(dot(gg, h, gh));
-      beta = gh / beta;
-      LSMF_TRY(dir_async<T>(d, h, beta, n, st));
-      old_alpha = alpha;
+      LSMF_CUDA(cudaMemcpyAsync(A.data(), ha + (k - batch), batch * sizeof(double), cudaMemcpyDeviceToHost, st));
+      LSMF_CUDA(cudaMemcpyAsync(Bt.data(), hb + (k - batch), batch * sizeof(double), cudaMemcpyDeviceToHost, st));
+      LSMF_CUDA(cudaMemcpyAsync(Rs.data(), hr + (k - batch), batch * sizeof(double), cudaMemcpyDeviceToHost, st));
+      LSMF_CUDA(cudaStreamSynchronize(st));
+      for (int j = 0; j < batch && !done; ++j) {
+        ++its;
+        const double alpha = A[j];
+        if (its > 1) {
+          dT.push_back(1.0 / alpha + prev_beta / prev_alpha);
+          oT.push_back(std::sqrt(prev_beta) / prev_alpha);
+        } else {
+          dT.push_back(1.0 / alpha);
+        }
+        if (std::sqrt(Rs[j]) <= tol || its >= max_it) done = true;
+        prev_beta = Bt[j];
+        prev_alpha = alpha;
+      }
     }
   }
   emin = emax = 1.0;
@@ -166,21 +186,25 @@ lsmf_status chebyshev_run(lsmf_gmg *g, int l, bool zero_start) {
   T *x = (T *)GL.x.ptr, *xold = (T *)GL.xold.ptr, *b = (T *)GL.b.ptr, *r = (T *)GL.r.ptr;
   const T *invd = (const T *)op->d_inv_diag.ptr;
   const lsmf_cheb &c = GL.cheb;
+  const uint8_t *cm = op->L().d_cmask.ptr;
+  // r is kept at zero between the steps by the update kernels
   if (zero_start) {
     LSMF_TRY(cheb_zero_async<T>(x, b, invd, c.theta, n, st));
+    LSMF_CUDA(cudaMemsetAsync(r, 0, n * sizeof(T), st));
   } else {
-    LSMF_TRY(launch_apply(op, r, x, LSMF_MASK_DEFAULT, false));
-    LSMF_TRY(cheb_first_async<T>(x, xold, b, r, invd, c.theta, n, st));
+    LSMF_CUDA(cudaMemsetAsync(r, 0, n * sizeof(T), st));
+    LSMF_TRY(launch_apply_cells(op, r, x));
+    LSMF_TRY(cheb_first_async<T>(x, xold, b, r, invd, cm, c.theta, n, st));
   }
   if (c.degree < 2 || std::fabs(c.delta) < 1e-40) return LSMF_OK;
   double rhok = c.delta / c.theta;
   const double sigma = c.theta / c.delta;
   for (int k = 0; k < c.degree - 1; ++k) {
-    LSMF_TRY(launch_apply(op, r, x, LSMF_MASK_DEFAULT, false));
+    LSMF_TRY(launch_apply_cells(op, r, x));
     const double rhokp = 1. / (2. * sigma - rhok);
     const double f1 = rhokp * rhok, f2 = 2. * rhokp / c.delta;
     rhok = rhokp;
-    LSMF_TRY(cheb_step_async<T>(x, xold, b, r, invd, f1, f2, !(zero_start && k == 0), n, st));
+    LSMF_TRY(cheb_step_async<T>(x, xold, b, r, invd, cm, f1, f2, !(zero_start && k == 0), n, st));
   }
   return LSMF_OK;
 }
@@ -246,7 +270,16 @@ lsmf_status gmg_vmult_impl(lsmf_gmg *g, double *dst, const double *src) {
 
 using namespace lsmf;
 
+static void drop_graph(lsmf_gmg *g) {
+  if (g->vexec) cudaGraphExecDestroy(g->vexec);
+  g->vexec = nullptr;
+  g->vsrc = nullptr;
+  g->vdst = nullptr;
+}
+
 lsmf_gmg::~lsmf_gmg() {
+  drop_graph(this);
+  if (cap_stream) cudaStreamDestroy(cap_stream);
   for (auto &GL : levels) lsmf_operator_destroy(GL.op);
 }
 
@@ -298,18 +331,56 @@ lsmf_status lsmf_gmg_set_material(lsmf_gmg *g, const double *mu, double nu) {
     LSMF_TRY(lsmf_operator_set_material(g->levels[l].op, ml.data(), nu));
   }
   g->ready = false;
+  drop_graph(g);
   return LSMF_OK;
 }
 
 lsmf_status lsmf_gmg_setup(lsmf_gmg *g, const double *d_u) {
   if (!g || !d_u) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  drop_graph(g);
   return g->desc.precision == LSMF_FP64 ? gmg_setup_impl<double>(g, d_u) : gmg_setup_impl<float>(g, d_u);
+}
+
+lsmf_status lsmf_gmg_set_option(lsmf_gmg *g, int option, int value) {
+  if (!g) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  if (option == LSMF_GMG_OPT_GRAPH) {
+    g->use_graph = value != 0;
+    drop_graph(g);
+    return LSMF_OK;
+  }
+  set_error("unknown option");
+  return LSMF_ERR_INVALID_ARG;
 }
 
 lsmf_status lsmf_gmg_vmult(lsmf_gmg *g, double *dst, const double *src) {
   if (!g || !dst || !src) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
   if (!g->ready) { set_error("lsmf_gmg_setup has not been called"); return LSMF_ERR_NOT_INITIALIZED; }
-  return g->desc.precision == LSMF_FP64 ? gmg_vmult_impl<double>(g, dst, src) : gmg_vmult_impl<float>(g, dst, src);
+  auto run = [&]() {
+    return g->desc.precision == LSMF_FP64 ? gmg_vmult_impl<double>(g, dst, src) : gmg_vmult_impl<float>(g, dst, src);
+  };
+  if (!g->use_graph) return run();
+  if (!g->vexec || g->vsrc != src || g->vdst != dst) {
+    // capture the V-cycle (a fixed sequence of launches once the Chebyshev
+    // coefficients are known) on a private stream, then replay it
+    drop_graph(g);
+    if (!g->cap_stream) LSMF_CUDA(cudaStreamCreateWithFlags(&g->cap_stream, cudaStreamNonBlocking));
+    const cudaStream_t user = g->stream;
+    lsmf_gmg_set_stream(g, g->cap_stream);
+    LSMF_CUDA(cudaStreamBeginCapture(g->cap_stream, cudaStreamCaptureModeRelaxed));
+    const lsmf_status s = run();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(g->cap_stream, &graph);
+    lsmf_gmg_set_stream(g, user);
+    if (s != LSMF_OK) { if (graph) cudaGraphDestroy(graph); return s; }
+    if (e != cudaSuccess) { set_error(std::string("V-cycle capture: ") + cudaGetErrorString(e)); return LSMF_ERR_CUDA; }
+    const cudaError_t ei = cudaGraphInstantiate(&g->vexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) { g->vexec = nullptr; set_error(std::string("V-cycle graph: ") + cudaGetErrorString(ei)); return LSMF_ERR_CUDA; }
+    g->vsrc = src;
+    g->vdst = dst;
+  }
+  LSMF_CUDA(cudaGraphLaunch(g->vexec, g->stream));
+  return LSMF_OK;
 }
 
 lsmf_status lsmf_gmg_level_info(const lsmf_gmg *g, int level, double *out6) {

@@ -854,6 +854,17 @@ lsmf_status launch_apply(const lsmf_op *op, void *dst, const void *src, unsigned
   return LSMF_OK;
 }
 
+lsmf_status launch_apply_cells(const lsmf_op *op, void *dst, const void *src) {
+  const Level &L = op->L();
+  const int v = variant_of(op);
+  const unsigned mask = LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD;
+  if (op->precision == LSMF_FP64)
+    return LSMF_DISPATCH_PQ(L.p, L.q,
+                            LSMF_DISPATCH_VAR(v, (run_apply<P_, Q_, double, V_>(op, (double *)dst, (const double *)src, mask))));
+  return LSMF_DISPATCH_PQ(L.p, L.q,
+                          LSMF_DISPATCH_VAR(v, (run_apply<P_, Q_, float, V_>(op, (float *)dst, (const float *)src, mask))));
+}
+
 // K g over the constrained columns: gather without zeroing, scatter skipping
 // constrained rows (dst zeroed first, no identity rows)
 lsmf_status launch_apply_inhomogeneous(const lsmf_op *op, void *dst, const void *g) {

@@ -96,7 +96,7 @@ struct Level {
   DevBuf<int> d_cell_nodes;     // packed with constraint bits
   DevBuf<double> d_X;
   DevBuf<int> d_constrained;
-  // cell colouring (8 colours) for deterministic scatter paths
+  DevBuf<uint8_t> d_cmask;      // per dof constrained flag
   int ncn() const { return (p + 1) * (p + 1) * (p + 1); }
   int nq() const { return q * q * q; }
   int n_dofs() const { return 3 * n_nodes; }
@@ -156,6 +156,9 @@ namespace lsmf {
 // kernels.cu launchers
 lsmf_status launch_cache(lsmf_op *op);
 lsmf_status launch_apply(const lsmf_op *op, void *dst, const void *src, unsigned mask, bool add);
+// only the cell loop: dst += sum of cell contributions (no zeroing, no
+// identity rows); callers fold those into their own element-wise kernels
+lsmf_status launch_apply_cells(const lsmf_op *op, void *dst, const void *src);
 lsmf_status launch_diagonal(lsmf_op *op);
 lsmf_status upload_basis_tables(const Basis &b);
 int table_components(int caching, int formulation, lsmf_precision precision);

@@ -192,6 +192,7 @@ lsmf_status level_constraints(const lsmf_mesh &M, Level &L) {
   }
   LSMF_TRY(L.d_cell_nodes.upload(packed.data(), packed.size()));
   LSMF_TRY(L.d_constrained.upload(L.constrained.data(), L.constrained.size()));
+  LSMF_TRY(L.d_cmask.upload(L.cmask.data(), L.cmask.size()));
   return LSMF_OK;
 }
 

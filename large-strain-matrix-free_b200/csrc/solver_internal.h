@@ -19,6 +19,12 @@ lsmf_status cg_update_async(double *x, double *g, const double *d, const double 
 lsmf_status cg_dir_async(double *d, const double *h, size_t n, const double *sc, int gh_new, int gh_old, bool first,
                          cudaStream_t st);
 template <typename T>
+lsmf_status eig_update_async(T *g, const T *h, size_t n, double *sc, int gh_slot, double *hist_alpha, double *hist_res2,
+                             int k, double *partial, cudaStream_t st);
+template <typename T>
+lsmf_status eig_dir_async(T *d, const T *h, size_t n, const double *sc, int gh_new, int gh_old, double *hist_beta,
+                          int k, cudaStream_t st);
+template <typename T>
 lsmf_status neg_residual_async(T *g, const T *ax, const T *b, size_t n, cudaStream_t st);
 template <typename T>
 lsmf_status jacobi_async(T *dst, const T *invd, const T *src, double omega, size_t n, cudaStream_t st);
@@ -34,12 +40,13 @@ template <typename T>
 lsmf_status copy_indexed_async(T *dst, const T *src, const int *idx, int n, cudaStream_t st);
 template <typename T>
 lsmf_status cheb_zero_async(T *x, const T *b, const T *invd, double theta, size_t n, cudaStream_t st);
+// r: cell contributions of A x only; identity rows added from cmask, r cleared
 template <typename T>
-lsmf_status cheb_first_async(T *x, T *xold, const T *b, const T *r, const T *invd, double theta, size_t n,
-                             cudaStream_t st);
+lsmf_status cheb_first_async(T *x, T *xold, const T *b, T *r, const T *invd, const uint8_t *cmask, double theta,
+                             size_t n, cudaStream_t st);
 template <typename T>
-lsmf_status cheb_step_async(T *x, T *xold, const T *b, const T *r, const T *invd, double f1, double f2, bool has_old,
-                            size_t n, cudaStream_t st);
+lsmf_status cheb_step_async(T *x, T *xold, const T *b, T *r, const T *invd, const uint8_t *cmask, double f1, double f2,
+                            bool has_old, size_t n, cudaStream_t st);
 template <typename T>
 lsmf_status restrict_add_async(const Level &C, const TransferMap &TM, const T *b, const T *r, T *coarse, cudaStream_t st);
 template <typename T>
@@ -85,8 +92,15 @@ struct lsmf_gmg {
   double nu = 0.3;
   lsmf::DevBuf<double> sc, partial;
   lsmf::DevBuf<char> eig_vecs;  // scratch for the eigenvalue CG (4 level vectors)
+  lsmf::DevBuf<double> eig_hist; // alpha / beta / residual history of the eigenvalue CG
   cudaStream_t stream = 0;
   bool ready = false;
+  // the V-cycle replayed as one CUDA graph (captured after each set-up)
+  bool use_graph = true;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t vexec = nullptr;
+  const double *vsrc = nullptr;
+  double *vdst = nullptr;
   size_t elem() const { return desc.precision == LSMF_FP64 ? 8 : 4; }
   ~lsmf_gmg();
 };

@@ -33,8 +33,8 @@ __global__ void dot_partial_kernel(const A *a, const B *b, size_t n, double *par
   }
 }
 
-// sums partial[0..n) in a fixed order into sc[slot]
-__global__ void reduce_final_kernel(const double *partial, int n, double *sc, int slot) {
+// sums partial[0..n) in a fixed order into *out
+__global__ void reduce_final_kernel(const double *partial, int n, double *out) {
   __shared__ double sh[32];
   double s = 0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) s += partial[i];
@@ -44,7 +44,7 @@ __global__ void reduce_final_kernel(const double *partial, int n, double *sc, in
   if (threadIdx.x < 32) {
     s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (threadIdx.x == 0) sc[slot] = s;
+    if (threadIdx.x == 0) *out = s;
   }
 }
 
@@ -76,6 +76,40 @@ __global__ void cg_dir_kernel(double *d, const double *h, size_t n, const double
   const double beta = first ? 0.0 : sc[gh_new] / sc[gh_old];
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     d[i] = beta * d[i] - h[i];
+}
+
+// eigenvalue CG (level precision): alpha = sc[gh] / sc[DH]; g += alpha h;
+// partial sums of g.g; alpha recorded in hist_alpha[k]
+template <typename T>
+__global__ void eig_update_kernel(T *g, const T *h, size_t n, const double *sc, int gh_slot, double *hist_alpha,
+                                  int k, double *partial) {
+  __shared__ double sh[RED_THREADS / 32];
+  const double alpha = sc[gh_slot] / sc[SC_DH];
+  if (blockIdx.x == 0 && threadIdx.x == 0) hist_alpha[k] = alpha;
+  double s = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double gi = (double)g[i] + alpha * (double)h[i];
+    g[i] = T(gi);
+    s += (double)g[i] * (double)g[i];
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  }
+}
+
+// d = beta d - h with beta = sc[gh_new] / sc[gh_old], recorded in hist_beta[k]
+template <typename T>
+__global__ void eig_dir_kernel(T *d, const T *h, size_t n, const double *sc, int gh_new, int gh_old, double *hist_beta,
+                               int k) {
+  const double beta = sc[gh_new] / sc[gh_old];
+  if (blockIdx.x == 0 && threadIdx.x == 0) hist_beta[k] = beta;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    d[i] = T(beta * (double)d[i] - (double)h[i]);
 }
 
 template <typename T>
@@ -128,21 +162,29 @@ __global__ void cheb_zero_kernel(T *x, const T *b, const T *invd, double inv_the
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     x[i] = T((double)invd[i] * (double)b[i] * inv_theta);
 }
+// r holds only the cell contributions of A x: the identity rows of the
+// constrained dofs are added here (A x = x there), and r is cleared for the
+// next cell loop, so a smoothing step is one cell-loop kernel plus this one
 template <typename T>
-__global__ void cheb_first_kernel(T *x, T *xold, const T *b, const T *r, const T *invd, double inv_theta, size_t n) {
+__global__ void cheb_first_kernel(T *x, T *xold, const T *b, T *r, const T *invd, const uint8_t *cmask,
+                                  double inv_theta, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const T xi = x[i];
+    const double ax = (double)r[i] + (cmask[i] ? (double)xi : 0.0);
+    r[i] = T(0);
     xold[i] = xi;
-    x[i] = T((double)xi + (double)invd[i] * ((double)b[i] - (double)r[i]) * inv_theta);
+    x[i] = T((double)xi + (double)invd[i] * ((double)b[i] - ax) * inv_theta);
   }
 }
 template <typename T>
-__global__ void cheb_step_kernel(T *x, T *xold, const T *b, const T *r, const T *invd, double f1, double f2,
-                                 int has_old, size_t n) {
+__global__ void cheb_step_kernel(T *x, T *xold, const T *b, T *r, const T *invd, const uint8_t *cmask, double f1,
+                                 double f2, int has_old, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const double xi = (double)x[i];
+    const double ax = (double)r[i] + (cmask[i] ? xi : 0.0);
+    r[i] = T(0);
     const double xo = has_old ? (double)xold[i] : 0.0;
-    const double xn = xi + f1 * (xi - xo) + f2 * (double)invd[i] * ((double)b[i] - (double)r[i]);
+    const double xn = xi + f1 * (xi - xo) + f2 * (double)invd[i] * ((double)b[i] - ax);
     xold[i] = T(xi);
     x[i] = T(xn);
   }
@@ -418,7 +460,7 @@ lsmf_status dot_async(const void *a, const void *b, bool fp32, size_t n, double 
   const int g = reduce_blocks();
   if (fp32) dot_partial_kernel<float, float><<<g, RED_THREADS, 0, st>>>((const float *)a, (const float *)b, n, partial);
   else dot_partial_kernel<double, double><<<g, RED_THREADS, 0, st>>>((const double *)a, (const double *)b, n, partial);
-  reduce_final_kernel<<<1, 1024, 0, st>>>(partial, g, sc, slot);
+  reduce_final_kernel<<<1, 1024, 0, st>>>(partial, g, sc + slot);
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
 }
@@ -427,10 +469,36 @@ lsmf_status cg_update_async(double *x, double *g, const double *d, const double 
                             double *partial, cudaStream_t st) {
   const int gr = reduce_blocks();
   cg_update_kernel<<<gr, RED_THREADS, 0, st>>>(x, g, d, h, n, sc, gh_slot, partial);
-  reduce_final_kernel<<<1, 1024, 0, st>>>(partial, gr, sc, SC_RES2);
+  reduce_final_kernel<<<1, 1024, 0, st>>>(partial, gr, sc + SC_RES2);
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
 }
+
+template <typename T>
+lsmf_status eig_update_async(T *g, const T *h, size_t n, double *sc, int gh_slot, double *hist_alpha, double *hist_res2,
+                             int k, double *partial, cudaStream_t st) {
+  const int gr = reduce_blocks();
+  eig_update_kernel<T><<<gr, RED_THREADS, 0, st>>>(g, h, n, sc, gh_slot, hist_alpha, k, partial);
+  reduce_final_kernel<<<1, 1024, 0, st>>>(partial, gr, hist_res2 + k);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+template lsmf_status eig_update_async<float>(float *, const float *, size_t, double *, int, double *, double *, int,
+                                             double *, cudaStream_t);
+template lsmf_status eig_update_async<double>(double *, const double *, size_t, double *, int, double *, double *, int,
+                                              double *, cudaStream_t);
+
+template <typename T>
+lsmf_status eig_dir_async(T *d, const T *h, size_t n, const double *sc, int gh_new, int gh_old, double *hist_beta,
+                          int k, cudaStream_t st) {
+  eig_dir_kernel<T><<<vec_grid(n), 256, 0, st>>>(d, h, n, sc, gh_new, gh_old, hist_beta, k);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+template lsmf_status eig_dir_async<float>(float *, const float *, size_t, const double *, int, int, double *, int,
+                                          cudaStream_t);
+template lsmf_status eig_dir_async<double>(double *, const double *, size_t, const double *, int, int, double *, int,
+                                           cudaStream_t);
 
 lsmf_status cg_dir_async(double *d, const double *h, size_t n, const double *sc, int gh_new, int gh_old, bool first,
                          cudaStream_t st) {
@@ -512,29 +580,29 @@ lsmf_status cheb_zero_async(T *x, const T *b, const T *invd, double theta, size_
   return LSMF_OK;
 }
 template <typename T>
-lsmf_status cheb_first_async(T *x, T *xold, const T *b, const T *r, const T *invd, double theta, size_t n,
-                             cudaStream_t st) {
-  cheb_first_kernel<T><<<vec_grid(n), 256, 0, st>>>(x, xold, b, r, invd, 1.0 / theta, n);
+lsmf_status cheb_first_async(T *x, T *xold, const T *b, T *r, const T *invd, const uint8_t *cmask, double theta,
+                             size_t n, cudaStream_t st) {
+  cheb_first_kernel<T><<<vec_grid(n), 256, 0, st>>>(x, xold, b, r, invd, cmask, 1.0 / theta, n);
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
 }
 template <typename T>
-lsmf_status cheb_step_async(T *x, T *xold, const T *b, const T *r, const T *invd, double f1, double f2, bool has_old,
-                            size_t n, cudaStream_t st) {
-  cheb_step_kernel<T><<<vec_grid(n), 256, 0, st>>>(x, xold, b, r, invd, f1, f2, has_old ? 1 : 0, n);
+lsmf_status cheb_step_async(T *x, T *xold, const T *b, T *r, const T *invd, const uint8_t *cmask, double f1, double f2,
+                            bool has_old, size_t n, cudaStream_t st) {
+  cheb_step_kernel<T><<<vec_grid(n), 256, 0, st>>>(x, xold, b, r, invd, cmask, f1, f2, has_old ? 1 : 0, n);
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
 }
 template lsmf_status cheb_zero_async<float>(float *, const float *, const float *, double, size_t, cudaStream_t);
 template lsmf_status cheb_zero_async<double>(double *, const double *, const double *, double, size_t, cudaStream_t);
-template lsmf_status cheb_first_async<float>(float *, float *, const float *, const float *, const float *, double, size_t,
-                                             cudaStream_t);
-template lsmf_status cheb_first_async<double>(double *, double *, const double *, const double *, const double *, double,
-                                              size_t, cudaStream_t);
-template lsmf_status cheb_step_async<float>(float *, float *, const float *, const float *, const float *, double, double,
-                                            bool, size_t, cudaStream_t);
-template lsmf_status cheb_step_async<double>(double *, double *, const double *, const double *, const double *, double,
-                                             double, bool, size_t, cudaStream_t);
+template lsmf_status cheb_first_async<float>(float *, float *, const float *, float *, const float *, const uint8_t *,
+                                             double, size_t, cudaStream_t);
+template lsmf_status cheb_first_async<double>(double *, double *, const double *, double *, const double *,
+                                              const uint8_t *, double, size_t, cudaStream_t);
+template lsmf_status cheb_step_async<float>(float *, float *, const float *, float *, const float *, const uint8_t *,
+                                            double, double, bool, size_t, cudaStream_t);
+template lsmf_status cheb_step_async<double>(double *, double *, const double *, double *, const double *,
+                                             const uint8_t *, double, double, bool, size_t, cudaStream_t);
 
 template <int P>
 static Prol1D<P> make_prol(const TransferMap &T) {

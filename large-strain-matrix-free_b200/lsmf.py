@@ -91,6 +91,7 @@ SIGNATURES = {
     "lsmf_gmg_vmult": (ctypes.c_int, [vp, vp, vp]),
     "lsmf_gmg_level_info": (ctypes.c_int, [vp, ctypes.c_int, dp]),
     "lsmf_gmg_set_stream": (ctypes.c_int, [vp, vp]),
+    "lsmf_gmg_set_option": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
     "lsmf_cg_solve": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, vp, vp, vp, ctypes.c_double,
                                      ctypes.c_int, ctypes.POINTER(SolveInfo)]),
     "lsmf_problem_create": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(vp)]),
@@ -327,6 +328,10 @@ class GMG:
 
     def vmult(self, dst, src):
         check(lib().lsmf_gmg_vmult(self.h, _dptr(dst), _dptr(src)))
+
+    def set_graph(self, enable):
+        """Replay the V-cycle as one CUDA graph (default) or launch kernel by kernel."""
+        check(lib().lsmf_gmg_set_option(self.h, 1, int(bool(enable))))
 
     def level_info(self, level):
         out = np.zeros(6)

@@ -53,6 +53,12 @@ def test_vcycle_matches_oracle(precision, caching, formulation):
     got, want = ddst.cpu().numpy(), og.vmult(src)
     tol = 1e-10 if precision == "fp64" else 1e-4
     assert np.max(np.abs(got - want)) <= tol * np.max(np.abs(want))
+    # the V-cycle replayed as a CUDA graph equals the kernel-by-kernel launch
+    # (up to the order of the floating-point atomics)
+    g.set_graph(False)
+    d2 = torch.empty_like(dsrc)
+    g.vmult(d2, dsrc)
+    assert torch.max(torch.abs(d2 - ddst)).item() <= (1e-12 if precision == "fp64" else 1e-5) * np.max(np.abs(got))
 
 
 def test_vcycle_cook_geometry():
