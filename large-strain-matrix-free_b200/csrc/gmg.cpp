@@ -176,14 +176,15 @@ void chebyshev_coefficients(lsmf_cheb &c, int degree, double range) {
   c.delta = 0.5 * (max_eig - alpha);
 }
 
-// PreconditionChebyshev::vmult (zero_start) / step
+// PreconditionChebyshev::vmult (zero_start) / step on the vectors x, b of
+// level l (the level's r and xold are the smoother's work vectors)
 template <typename T>
-lsmf_status chebyshev_run(lsmf_gmg *g, int l, bool zero_start) {
+lsmf_status chebyshev_run(lsmf_gmg *g, int l, T *x, const T *b, bool zero_start) {
   lsmf_gmg_level &GL = g->levels[l];
   lsmf_op *op = GL.op;
   const size_t n = (size_t)op->L().n_dofs();
   cudaStream_t st = g->stream;
-  T *x = (T *)GL.x.ptr, *xold = (T *)GL.xold.ptr, *b = (T *)GL.b.ptr, *r = (T *)GL.r.ptr;
+  T *xold = (T *)GL.xold.ptr, *r = (T *)GL.r.ptr;
   const T *invd = (const T *)op->d_inv_diag.ptr;
   const lsmf_cheb &c = GL.cheb;
   const uint8_t *cm = op->L().d_cmask.ptr;
@@ -209,21 +210,74 @@ lsmf_status chebyshev_run(lsmf_gmg *g, int l, bool zero_start) {
   return LSMF_OK;
 }
 
+// MGCoarseGridIterativeSolver (mf_elasticity.h:2116-2127): CG on level 0,
+// preconditioned by the level-0 Chebyshev smoother, ReductionControl with
+// max(m, 100) steps, absolute 1e-10, relative 1e-3, zero initial guess
+template <typename T>
+lsmf_status coarse_cg(lsmf_gmg *g) {
+  lsmf_gmg_level &GL = g->levels[0];
+  lsmf_op *op = GL.op;
+  const size_t n = (size_t)op->L().n_dofs();
+  cudaStream_t st = g->stream;
+  const bool fp32 = sizeof(T) == 4;
+  T *x = (T *)GL.x.ptr, *b = (T *)GL.b.ptr;
+  T *gg = (T *)g->eig_vecs.ptr, *h = gg + n, *d = h + n;
+  double *sc = g->sc.ptr, *part = g->partial.ptr;
+  auto dot = [&](const T *a, const T *c, double &out) -> lsmf_status {
+    LSMF_TRY(dot_async(a, c, fp32, n, part, sc, SC_TMP, st));
+    LSMF_CUDA(cudaMemcpyAsync(&out, sc + SC_TMP, sizeof(double), cudaMemcpyDeviceToHost, st));
+    LSMF_CUDA(cudaStreamSynchronize(st));
+    return LSMF_OK;
+  };
+  LSMF_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), st));
+  LSMF_CUDA(cudaMemsetAsync(gg, 0, n * sizeof(T), st));
+  LSMF_TRY(dir_async<T>(gg, b, 0.0, n, st));  // g = A 0 - b
+  double res2;
+  LSMF_TRY(dot(gg, gg, res2));
+  const double tol = std::max(1e-10, 1e-3 * std::sqrt(res2));
+  if (std::sqrt(res2) <= tol) return LSMF_OK;
+  const int max_it = std::max((int)n, 100);
+  LSMF_TRY(chebyshev_run<T>(g, 0, h, gg, true));
+  LSMF_CUDA(cudaMemsetAsync(d, 0, n * sizeof(T), st));
+  LSMF_TRY(dir_async<T>(d, h, 0.0, n, st));
+  double gh;
+  LSMF_TRY(dot(gg, h, gh));
+  for (int it = 1; it <= max_it; ++it) {
+    LSMF_TRY(launch_apply(op, h, d, LSMF_MASK_DEFAULT, false));
+    double dh;
+    LSMF_TRY(dot(d, h, dh));
+    const double alpha = gh / dh;
+    LSMF_TRY(axpy_async<T>(x, alpha, d, n, st));
+    LSMF_TRY(axpy_async<T>(gg, alpha, h, n, st));
+    LSMF_TRY(dot(gg, gg, res2));
+    if (std::sqrt(res2) <= tol || !(res2 == res2)) break;
+    LSMF_TRY(chebyshev_run<T>(g, 0, h, gg, true));
+    const double gh_old = gh;
+    LSMF_TRY(dot(gg, h, gh));
+    LSMF_TRY(dir_async<T>(d, h, gh / gh_old, n, st));
+  }
+  return LSMF_OK;
+}
+
 // Multigrid::level_v_step
 template <typename T>
 lsmf_status vcycle(lsmf_gmg *g, int l) {
-  if (l == 0) return chebyshev_run<T>(g, 0, true);  // MGCoarseGridApplySmoother
+  if (l == 0) {
+    if (!g->desc.coarse_chebyshev) return coarse_cg<T>(g);
+    // MGCoarseGridApplySmoother
+    return chebyshev_run<T>(g, 0, (T *)g->levels[0].x.ptr, (const T *)g->levels[0].b.ptr, true);
+  }
   lsmf_gmg_level &GL = g->levels[l], &GC = g->levels[l - 1];
   cudaStream_t st = g->stream;
   const lsmf_mesh &M = *g->mesh;
-  LSMF_TRY(chebyshev_run<T>(g, l, true));  // pre-smoothing (apply: zero start)
+  LSMF_TRY(chebyshev_run<T>(g, l, (T *)GL.x.ptr, (const T *)GL.b.ptr, true));  // pre-smoothing (apply)
   LSMF_TRY(launch_apply(GL.op, GL.r.ptr, GL.x.ptr, LSMF_MASK_DEFAULT, false));
   LSMF_CUDA(cudaMemsetAsync(GC.b.ptr, 0, (size_t)GC.op->L().n_dofs() * sizeof(T), st));
   LSMF_TRY(restrict_add_async<T>(*M.levels[l - 1], *M.transfer[l], (const T *)GL.b.ptr, (const T *)GL.r.ptr,
                                  (T *)GC.b.ptr, st));
   LSMF_TRY(vcycle<T>(g, l - 1));
   LSMF_TRY(prolongate_add_async<T>(*M.levels[l - 1], *M.transfer[l], (const T *)GC.x.ptr, (T *)GL.x.ptr, st));
-  LSMF_TRY(chebyshev_run<T>(g, l, false));  // post-smoothing (smooth: step)
+  LSMF_TRY(chebyshev_run<T>(g, l, (T *)GL.x.ptr, (const T *)GL.b.ptr, false));  // post-smoothing (step)
   return LSMF_OK;
 }
 
@@ -358,7 +412,9 @@ lsmf_status lsmf_gmg_vmult(lsmf_gmg *g, double *dst, const double *src) {
   auto run = [&]() {
     return g->desc.precision == LSMF_FP64 ? gmg_vmult_impl<double>(g, dst, src) : gmg_vmult_impl<float>(g, dst, src);
   };
-  if (!g->use_graph) return run();
+  // the CG coarse solver reads scalars on the host, so that V-cycle is not
+  // captured
+  if (!g->use_graph || !g->desc.coarse_chebyshev) return run();
   if (!g->vexec || g->vsrc != src || g->vdst != dst) {
     // capture the V-cycle (a fixed sequence of launches once the Chebyshev
     // coefficients are known) on a private stream, then replay it

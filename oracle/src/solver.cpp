@@ -348,6 +348,15 @@ template struct Chebyshev<double>;
 template <typename T>
 void GMG<T>::vcycle(int l, std::vector<T> &x, const std::vector<T> &b) const {
   const Level &L = levels[l];
+  if (l == 0 && coarse_cg) {
+    const size_t n = b.size();
+    std::fill(x.begin(), x.end(), T(0));
+    auto Am = [&](std::vector<T> &dst, const std::vector<T> &src) { L.op.vmult(dst.data(), src.data()); };
+    auto Pm = [&](std::vector<T> &dst, const std::vector<T> &src) { L.cheb.run(dst, src, true); };
+    const int max_it = std::max((int)n, 100);
+    cg_solve(Am, Pm, x, b, max_it, 1e-10, 1e-3, nullptr, nullptr, nullptr, nullptr);
+    return;
+  }
   if (l == 0) { L.cheb.run(x, b, true); return; }   // MGCoarseGridApplySmoother
   L.cheb.run(x, b, true);                           // pre-smoothing: apply()
   std::vector<T> t(b.size());
@@ -491,6 +500,7 @@ void setup_gmg(const NewtonParams &prm, const std::vector<Mesh> &meshes, const B
     auto &L = gmg.levels[l];
     L.op.cache(lu[l].data());
     L.op.compute_diagonal();
+    gmg.coarse_cg = !prm.coarse_chebyshev;
     if (l == 0 && prm.coarse_chebyshev)
       L.cheb.setup(L.op, L.op.inv_diag, 0, 1e-3,
                    prm.coarse_accurate_eig ? L.mesh.n_dofs() : prm.cheb_eig_its);

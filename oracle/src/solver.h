@@ -44,6 +44,10 @@ struct GMG {
     Transfer transfer;  // from level-1 to this level (unused on level 0)
   };
   std::vector<Level> levels;
+  // coarse solve: Chebyshev "solver" mode, or (coarse_cg) CG preconditioned
+  // by the level-0 Chebyshev smoother to a 1e-3 reduction
+  // (MGCoarseGridIterativeSolver, mf_elasticity.h:2116-2127)
+  bool coarse_cg = false;
   void vcycle(int l, std::vector<T> &x, const std::vector<T> &b) const;
   void vmult(std::vector<double> &dst, const std::vector<double> &src) const;
 };

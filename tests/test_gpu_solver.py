@@ -119,3 +119,24 @@ def test_cg_reports_non_convergence():
     x = torch.zeros_like(b)
     info = lsmf.cg_solve(op, x, b, 1e-14, 3, "none")
     assert not info["converged"] and info["status"] == 5 and info["iterations"] == 3
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_vcycle_coarse_cg_matches_oracle(precision):
+    """'MF Chebyshev coarse = false': CG preconditioned by the level-0 Chebyshev
+    smoother to a 1e-3 reduction (MGCoarseGridIterativeSolver)."""
+    gm, mu, u, dirichlet, (lo, hi), rng = _problem("tensor4", 1)
+    og = O.GMG(O.GEOM_BOX, (1, 1, 1), 2, lo, hi, 1.0, 2, 3, "tensor4", 1, precision == "fp32", mu, 0.3,
+               dirichlet, u, coarse_chebyshev=False)
+    g = lsmf.GMG(gm, "tensor4", 1, precision, coarse_chebyshev=False)
+    g.set_material(mu, 0.3)
+    g.setup(torch.tensor(u, device="cuda"))
+    assert g.level_info(0)[2] == og.level_info(0)[2] == 5
+    src = rng.uniform(-1, 1, u.size)
+    src[gm.constraint_mask() == 1] = 0
+    dsrc = torch.tensor(src, device="cuda")
+    ddst = torch.empty_like(dsrc)
+    g.vmult(ddst, dsrc)
+    want = og.vmult(src)
+    tol = 1e-9 if precision == "fp64" else 1e-4
+    assert np.max(np.abs(ddst.cpu().numpy() - want)) <= tol * np.max(np.abs(want))
