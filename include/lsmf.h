@@ -41,7 +41,9 @@ typedef enum {
 typedef enum {
   LSMF_CACHE_SCALAR = 0,
   LSMF_CACHE_TENSOR2 = 1,
-  LSMF_CACHE_TENSOR4 = 2
+  LSMF_CACHE_TENSOR4 = 2,
+  LSMF_CACHE_SCALAR_REFERENTIAL = 3, /* reference frame, mf_nh_operator.h:1255-1400 (formulation 1) */
+  LSMF_CACHE_TENSOR4_NS = 4          /* dP/dF, reference frame, mf_nh_operator.h:563-582 (formulation 1) */
 } lsmf_caching;
 
 typedef enum { LSMF_FP64 = 0, LSMF_FP32 = 1 } lsmf_precision;
@@ -141,9 +143,12 @@ lsmf_status lsmf_operator_set_option(lsmf_op *op, int option, int value);
 /* the CUDA stream every operator call is ordered on (cudaStream_t) */
 lsmf_status lsmf_operator_set_stream(lsmf_op *op, void *stream);
 /* copy a cache table to the host for checking: which = 0 scalar / c1,
- * 1 second scalar, 2 tau/J (6 per qp), 3 tensor4 (36 per qp), 4 Eulerian
- * inverse Jacobian (9 per qp), 5 Eulerian JxW; layout [cell][qp][comp]
- * converted to double.  Returns the number of doubles in *count. */
+ * 1 second scalar, 2 tau/J (6 per qp), 3 tensor4 (36 per qp), 4 inverse
+ * Jacobian (9 per qp; Eulerian, or referential for scalar_referential and
+ * tensor4_ns), 5 JxW (same frame), 6 scalar_referential displacement values
+ * (3 per qp), 7 tensor4_ns dP/dF (81 per qp, index ((i*3+j)*3+k)*3+l);
+ * layout [cell][qp][comp] converted to double.  Returns the number of
+ * doubles in *count. */
 lsmf_status lsmf_operator_get_table(lsmf_op *op, int which, double *host, size_t *count);
 
 /* ---- geometric multigrid preconditioner (mf_elasticity.h:1712-2241) ---- */

@@ -108,7 +108,8 @@ lsmf_status lsmf_operator_create(lsmf_mesh *m, int level, lsmf_caching caching, 
   *out = nullptr;
   if (level < 0) level = (int)m->levels.size() - 1;
   if (level >= (int)m->levels.size()) { set_error("bad level"); return LSMF_ERR_INVALID_ARG; }
-  if (caching != LSMF_CACHE_SCALAR && caching != LSMF_CACHE_TENSOR2 && caching != LSMF_CACHE_TENSOR4) {
+  if (caching != LSMF_CACHE_SCALAR && caching != LSMF_CACHE_TENSOR2 && caching != LSMF_CACHE_TENSOR4 &&
+      caching != LSMF_CACHE_SCALAR_REFERENTIAL && caching != LSMF_CACHE_TENSOR4_NS) {
     set_error("Unknown caching");  // mf_nh_operator.h:439-442
     return LSMF_ERR_UNKNOWN_CACHING;
   }
@@ -244,13 +245,16 @@ lsmf_status lsmf_operator_get_table(lsmf_op *op, int which, double *host, size_t
   const int nq = L.nq(), nc = op->ncomp;
   int c0 = 0, nk = 0;
   const bool t4 = op->caching == LSMF_CACHE_TENSOR4, t2 = op->caching == LSMF_CACHE_TENSOR2;
+  const bool sr = op->caching == LSMF_CACHE_SCALAR_REFERENTIAL, ns = op->caching == LSMF_CACHE_TENSOR4_NS;
   switch (which) {
-    case 0: if (t4) { set_error("no scalar table"); return LSMF_ERR_INVALID_ARG; } c0 = 10; nk = 1; break;
+    case 0: if (t4 || ns) { set_error("no scalar table"); return LSMF_ERR_INVALID_ARG; } c0 = 10; nk = 1; break;
     case 1: if (!t2) { set_error("no second scalar table"); return LSMF_ERR_INVALID_ARG; } c0 = 11; nk = 1; break;
     case 2: if (!t2 && !t4) { set_error("no tensor2 table"); return LSMF_ERR_INVALID_ARG; } c0 = t4 ? 10 : 12; nk = 6; break;
     case 3: if (!t4) { set_error("no tensor4 table"); return LSMF_ERR_INVALID_ARG; } c0 = 16; nk = 36; break;
     case 4: c0 = 0; nk = 9; break;
     case 5: c0 = 9; nk = 1; break;
+    case 6: if (!sr) { set_error("no displacement table"); return LSMF_ERR_INVALID_ARG; } c0 = 11; nk = 3; break;
+    case 7: if (!ns) { set_error("no tensor4_ns table"); return LSMF_ERR_INVALID_ARG; } c0 = 10; nk = 81; break;
     default: set_error("bad table id"); return LSMF_ERR_INVALID_ARG;
   }
   const size_t n = (size_t)L.n_cells * nq * nk;

@@ -13,18 +13,28 @@
 
 namespace lsmf {
 
-enum Variant { VAR_TENSOR4 = 0, VAR_TENSOR2 = 1, VAR_SCALAR_F1 = 2, VAR_SCALAR_F0 = 3 };
+enum Variant {
+  VAR_TENSOR4 = 0, VAR_TENSOR2 = 1, VAR_SCALAR_F1 = 2, VAR_SCALAR_F0 = 3,
+  VAR_SCALAR_REF = 4,  // scalar_referential
+  VAR_TENSOR4_NS = 5   // tensor4_ns (dP/dF)
+};
+__host__ __device__ constexpr bool variant_referential(int v) { return v == VAR_SCALAR_REF || v == VAR_TENSOR4_NS; }
 
-// Record layout per cell: [comp][qp]; first 10 components are the Eulerian
-// metric (inverse Jacobian row-major, JxW) in every variant.
+// Record layout per cell: [comp][qp]; the first 10 components are the metric
+// (inverse Jacobian row-major, JxW) of the frame the variant integrates in:
+// Eulerian for tensor4 / tensor2 / scalar, reference for scalar_referential
+// and tensor4_ns.  Then: tensor4 tau/J (6) + C (36); tensor2 c1, c2, tau/J
+// (6); scalar c + reference inverse Jacobian (9); scalar_referential c + u at
+// the point (3); tensor4_ns dP/dF (81) + 1 pad (16-byte records).
 constexpr int C_JINV = 0, C_JXW = 9, C_VAR = 10;
 __host__ __device__ constexpr int variant_ncomp(int v) {
-  return v == VAR_TENSOR4 ? 52 : v == VAR_TENSOR2 ? 18 : 20;
+  return v == VAR_TENSOR4 ? 52 : v == VAR_TENSOR2 ? 18 : v == VAR_SCALAR_REF ? 14 : v == VAR_TENSOR4_NS ? 92 : 20;
 }
 
 template <int P, int Q>
 struct Tab {
   double N[Q][P + 1], D[Q][P + 1], w[Q];
+  double Dc[Q][Q];  // collocation derivative on the Gauss points
 };
 
 // 1D tables in the arithmetic type, passed by value as a kernel parameter:
@@ -33,7 +43,37 @@ struct Tab {
 template <int P, int Q, typename T>
 struct TabT {
   T N[Q][P + 1], D[Q][P + 1];
+  T Dc[Q][Q];  // collocation derivative on the Gauss points
 };
+
+// scalar_referential: F = I + Grad u from the displacement stored at the
+// points of the cell record (collocation derivative, the
+// FEEvaluationImplCollocation step of mf_nh_operator.h:1271-1300) and the
+// reference inverse Jacobian
+template <int Q, typename T, typename DC>
+__device__ __forceinline__ void collocation_F(const T *__restrict__ rec, int q, const DC &Dc, const T Ji[3][3],
+                                              T F[3][3]) {
+  constexpr int NQ = Q * Q * Q;
+  const int qx = q % Q, qy = (q / Q) % Q, qz = q / (Q * Q);
+  T G[3][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const T *u = rec + (C_VAR + 1 + c) * NQ;
+    T gx = 0, gy = 0, gz = 0;
+#pragma unroll
+    for (int m = 0; m < Q; ++m) {
+      gx += T(Dc[qx][m]) * u[(qz * Q + qy) * Q + m];
+      gy += T(Dc[qy][m]) * u[(qz * Q + m) * Q + qx];
+      gz += T(Dc[qz][m]) * u[(m * Q + qy) * Q + qx];
+    }
+    G[c][0] = gx; G[c][1] = gy; G[c][2] = gz;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      F[c][d] = G[c][0] * Ji[0][d] + G[c][1] * Ji[1][d] + G[c][2] * Ji[2][d] + (c == d ? T(1) : T(0));
+}
 
 // Sum factorisation with one 1D line per lane ("row" sweeps).  Each sweep
 // maps lane -> row of the tensor it produces and unrolls the 1D contraction
@@ -448,6 +488,53 @@ __device__ __forceinline__ void physics(const T g[3][3], const T *__restrict__ r
       Qm[i][j] += v;
       if (i != j) Qm[j][i] += v;
     }
+  } else if (VAR == VAR_TENSOR4_NS) {
+    // out_ij = A_ijkl Grad v_kl (double_contract<2,0,3,1>, mf_nh_operator.h:1441-1455)
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        T a = 0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+          for (int l = 0; l < 3; ++l) a += rec[(C_VAR + ((i * 3 + j) * 3 + k) * 3 + l) * NQ] * g[k][l];
+        Qm[i][j] = a;
+      }
+  } else if (VAR == VAR_SCALAR_REF) {
+    // mf_nh_operator.h:1255-1400: g = Grad v; grad_x v = Grad v F^-1; the
+    // scalar-variant physics; submitted as (jc + grad_x v tau) F^-T
+    const T c = rec[C_VAR * NQ];
+    T Fi[3][3];
+    inv3(st.F, Fi);
+    T gx[3][3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int e = 0; e < 3; ++e) gx[d][e] = g[d][0] * Fi[0][e] + g[d][1] * Fi[1][e] + g[d][2] * Fi[2][e];
+    T tau[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const T b = st.F[i][0] * st.F[j][0] + st.F[i][1] * st.F[j][1] + st.F[i][2] * st.F[j][2];
+        tau[i][j] = mu * b - (i == j ? c : T(0));
+      }
+    const T trx = gx[0][0] + gx[1][1] + gx[2][2];
+    T qd[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        T v = c * (gx[i][j] + gx[j][i]);
+        if (i == j) v += T(2) * lambda * trx;
+        v += gx[i][0] * tau[0][j] + gx[i][1] * tau[1][j] + gx[i][2] * tau[2][j];
+        qd[i][j] = v;
+      }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) Qm[i][j] = qd[i][0] * Fi[j][0] + qd[i][1] * Fi[j][1] + qd[i][2] * Fi[j][2];
   } else if (VAR == VAR_SCALAR_F1) {
     // mf_nh_operator.h:1182-1254: tau = mu b - c I, jc = 2c sym + 2 lambda tr I
     const T c = rec[C_VAR * NQ];

@@ -161,9 +161,17 @@ __global__ void __launch_bounds__(256) cache_kernel(KArgs<T> a, Tab<P, Q> tab) {
       inv3(Jr, Jri);
       const double dc = inv3(Jc, Jci);
       T *r = rec + q;
+      if (variant_referential(VAR)) {
+        // scalar_referential / tensor4_ns integrate in the reference frame
+        const double dr = det3(Jr);
 #pragma unroll
-      for (int i = 0; i < 9; ++i) r[(C_JINV + i) * NQ] = T(Jci[i / 3][i % 3]);
-      r[C_JXW * NQ] = T(dc * w);
+        for (int i = 0; i < 9; ++i) r[(C_JINV + i) * NQ] = T(Jri[i / 3][i % 3]);
+        r[C_JXW * NQ] = T(dr * w);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) r[(C_JINV + i) * NQ] = T(Jci[i / 3][i % 3]);
+        r[C_JXW * NQ] = T(dc * w);
+      }
       // F = I + Grad u (reference configuration, mf_nh_operator.h:462-476)
       double F[3][3];
 #pragma unroll
@@ -181,6 +189,37 @@ __global__ void __launch_bounds__(256) cache_kernel(KArgs<T> a, Tab<P, Q> tab) {
         continue;
       }
       const double scalar = mu - 2.0 * lambda * log(det_F);
+      if (VAR == VAR_SCALAR_REF) {
+        // c and the displacement values at the point (phi_reference.begin_values())
+        r[C_VAR * NQ] = T(scalar);
+        const int qx = q % Q, qy = (q / Q) % Q, qz = q / (Q * Q);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          double v = 0;
+          for (int kz = 0; kz <= P; ++kz)
+            for (int jy = 0; jy <= P; ++jy)
+              for (int ix = 0; ix <= P; ++ix)
+                v += sN[qx * (P + 1) + ix] * sN[qy * (P + 1) + jy] * sN[qz * (P + 1) + kz] *
+                     V[c * NN + (kz * (P + 1) + jy) * (P + 1) + ix];
+          r[(C_VAR + 1 + c) * NQ] = T(v);
+        }
+        continue;
+      }
+      if (VAR == VAR_TENSOR4_NS) {
+        // 2 lambda F^-T (x) F^-T + (mu - 2 lambda ln J) F^-T_il F^-1_jk + mu I_ik I_jl
+        double Fi[3][3];
+        inv3(F, Fi);
+        const double lnJ = log(det_F);
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j)
+            for (int k = 0; k < 3; ++k)
+              for (int l = 0; l < 3; ++l)
+                r[(C_VAR + ((i * 3 + j) * 3 + k) * 3 + l) * NQ] =
+                    T(2.0 * lambda * Fi[j][i] * Fi[l][k] + (mu - 2.0 * lambda * lnJ) * Fi[l][i] * Fi[j][k] +
+                      (i == k && j == l ? mu : 0.0));
+        r[(C_VAR + 81) * NQ] = T(0);
+        continue;
+      }
       const double idet = 1.0 / det_F;
       double tau[6];
 #pragma unroll
@@ -252,7 +291,7 @@ __global__ void __launch_bounds__(256) apply_kernel(KArgs<T> a, Tab<P, Q> tab) {
           for (int e = 0; e < 3; ++e) G[l][c][e] = T(0);
     }
     T mu = 0, lambda = 0, kappa = 0;
-    if (SCALAR) material<T>(a.mu[cell], a.nu, mu, lambda, kappa);
+    if (SCALAR || VAR == VAR_SCALAR_REF) material<T>(a.mu[cell], a.nu, mu, lambda, kappa);
     T H[QPL][3][3];
 #pragma unroll
     for (int l = 0; l < QPL; ++l) {
@@ -282,6 +321,10 @@ __global__ void __launch_bounds__(256) apply_kernel(KArgs<T> a, Tab<P, Q> tab) {
 #pragma unroll
           for (int d = 0; d < 3; ++d)
             st.F[c][d] = GU[l][c][0] * Jr[0][d] + GU[l][c][1] * Jr[1][d] + GU[l][c][2] * Jr[2][d] + (c == d ? T(1) : T(0));
+        st.det = det3(st.F);
+      }
+      if (VAR == VAR_SCALAR_REF) {
+        collocation_F<Q>(rec, q, tab.Dc, Ji, st.F);
         st.det = det3(st.F);
       }
       T Qm[3][3];
@@ -424,7 +467,7 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
       rec = a.table + (size_t)cell * rec_elems;
     }
     T mu = 0, lambda = 0, kappa = 0;
-    if (SCALAR) material<T>(a.mu[cell], a.nu, mu, lambda, kappa);
+    if (SCALAR || VAR == VAR_SCALAR_REF) material<T>(a.mu[cell], a.nu, mu, lambda, kappa);
     T H[QPL][3][3];
 #pragma unroll
     for (int l = 0; l < QPL; ++l) {
@@ -454,6 +497,10 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
 #pragma unroll
           for (int d = 0; d < 3; ++d)
             st.F[c][d] = GU[l][c][0] * Jr[0][d] + GU[l][c][1] * Jr[1][d] + GU[l][c][2] * Jr[2][d] + (c == d ? T(1) : T(0));
+        st.det = det3(st.F);
+      }
+      if (VAR == VAR_SCALAR_REF) {
+        collocation_F<Q>(rec, q, tab.Dc, Ji, st.F);
         st.det = det3(st.F);
       }
       T Qm[3][3];
@@ -521,15 +568,19 @@ __global__ void __launch_bounds__(128) diagonal_kernel(KArgs<T> a, Tab<P, Q> tab
       S::eval(sN, sD, V, A, B, lane, GU);
     }
     T mu = 0, lambda = 0, kappa = 0;
-    if (SCALAR) material<T>(a.mu[cell], a.nu, mu, lambda, kappa);
+    if (SCALAR || VAR == VAR_SCALAR_REF) material<T>(a.mu[cell], a.nu, mu, lambda, kappa);
 #pragma unroll
     for (int l = 0; l < QPL; ++l) {
       const int q = lane + 32 * l;
       if (q >= NQ) continue;
       const T *r = rec + q;
       const T jxw = r[C_JXW * NQ];
+      T Ji[3][3];
 #pragma unroll
-      for (int i = 0; i < 9; ++i) Jq[q * 9 + i] = r[(C_JINV + i) * NQ];
+      for (int i = 0; i < 9; ++i) {
+        Jq[q * 9 + i] = r[(C_JINV + i) * NQ];
+        Ji[i / 3][i % 3] = r[(C_JINV + i) * NQ];
+      }
       ScalarState<T> st;
       if (SCALAR) {
         T Jr[3][3];
@@ -540,6 +591,10 @@ __global__ void __launch_bounds__(128) diagonal_kernel(KArgs<T> a, Tab<P, Q> tab
 #pragma unroll
           for (int d = 0; d < 3; ++d)
             st.F[c][d] = GU[l][c][0] * Jr[0][d] + GU[l][c][1] * Jr[1][d] + GU[l][c][2] * Jr[2][d] + (c == d ? T(1) : T(0));
+        st.det = det3(st.F);
+      }
+      if (VAR == VAR_SCALAR_REF) {
+        collocation_F<Q>(rec, q, tab.Dc, Ji, st.F);
         st.det = det3(st.F);
       }
 #pragma unroll
@@ -627,11 +682,13 @@ int num_sms() {
 template <int P, int Q, typename T>
 TabT<P, Q, T> make_tabt(const Basis &b) {
   TabT<P, Q, T> t;
-  for (int k = 0; k < Q; ++k)
+  for (int k = 0; k < Q; ++k) {
     for (int i = 0; i <= P; ++i) {
       t.N[k][i] = T(b.N[k * (P + 1) + i]);
       t.D[k][i] = T(b.D[k * (P + 1) + i]);
     }
+    for (int m = 0; m < Q; ++m) t.Dc[k][m] = T(b.Dc[k * Q + m]);
+  }
   return t;
 }
 
@@ -644,6 +701,7 @@ Tab<P, Q> make_tab(const Basis &b) {
       t.D[k][i] = b.D[k * (P + 1) + i];
     }
     t.w[k] = b.qw[k];
+    for (int m = 0; m < Q; ++m) t.Dc[k][m] = b.Dc[k * Q + m];
   }
   return t;
 }
@@ -675,6 +733,8 @@ inline int warps_for_budget(size_t warp_bytes, int max_warps, size_t budget) {
 int variant_of(const lsmf_op *op) {
   if (op->caching == LSMF_CACHE_TENSOR4) return VAR_TENSOR4;
   if (op->caching == LSMF_CACHE_TENSOR2) return VAR_TENSOR2;
+  if (op->caching == LSMF_CACHE_SCALAR_REFERENTIAL) return VAR_SCALAR_REF;
+  if (op->caching == LSMF_CACHE_TENSOR4_NS) return VAR_TENSOR4_NS;
   return op->formulation == 0 ? VAR_SCALAR_F0 : VAR_SCALAR_F1;
 }
 
@@ -732,7 +792,7 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask) {
   // defaults measured on B200 at 64^3 Q2 (ring depth, warps per block):
   // tensor4 streams 52 values per point and wants the bulk-copy ring;
   // tensor2 and scalar are latency / FP64 bound and run best on plain loads
-  int stages = op->stages >= 0 ? op->stages : (VAR == VAR_TENSOR4 ? 1 : 0);
+  int stages = op->stages >= 0 ? op->stages : ((VAR == VAR_TENSOR4 || VAR == VAR_TENSOR4_NS) ? 1 : 0);
   const int max_warps = op->max_warps > 0 ? op->max_warps : (VAR == VAR_TENSOR2 ? 8 : 4);
   if (rec_bytes % 16 != 0) stages = 0;
   // fewer stages when the ring would leave fewer than 4 warps per block
@@ -803,6 +863,8 @@ lsmf_status run_diag(lsmf_op *op, T *diag) {
       case VAR_TENSOR4: { constexpr int V_ = VAR_TENSOR4; return __VA_ARGS__; }       \
       case VAR_TENSOR2: { constexpr int V_ = VAR_TENSOR2; return __VA_ARGS__; }       \
       case VAR_SCALAR_F1: { constexpr int V_ = VAR_SCALAR_F1; return __VA_ARGS__; }   \
+      case VAR_SCALAR_REF: { constexpr int V_ = VAR_SCALAR_REF; return __VA_ARGS__; } \
+      case VAR_TENSOR4_NS: { constexpr int V_ = VAR_TENSOR4_NS; return __VA_ARGS__; } \
       default: { constexpr int V_ = VAR_SCALAR_F0; return __VA_ARGS__; }             \
     }                                                                                 \
   }()
@@ -816,6 +878,8 @@ int table_components(int caching, int formulation, lsmf_precision precision) {
   (void)formulation;
   if (caching == LSMF_CACHE_TENSOR4) return variant_ncomp(VAR_TENSOR4);
   if (caching == LSMF_CACHE_TENSOR2) return variant_ncomp(VAR_TENSOR2) + (precision == LSMF_FP32 ? 2 : 0);
+  if (caching == LSMF_CACHE_SCALAR_REFERENTIAL) return variant_ncomp(VAR_SCALAR_REF) + (precision == LSMF_FP32 ? 2 : 0);
+  if (caching == LSMF_CACHE_TENSOR4_NS) return variant_ncomp(VAR_TENSOR4_NS);
   return variant_ncomp(VAR_SCALAR_F1);
 }
 

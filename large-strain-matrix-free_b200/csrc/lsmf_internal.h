@@ -39,6 +39,7 @@ constexpr int NODE_MASK = (1 << NODE_BITS) - 1;
 struct Basis {
   int p = 0, q = 0;
   std::vector<double> nodes, qpts, qw, N, D;  // N, D: [q][p+1]
+  std::vector<double> Dc;  // [q][q]: derivative of the Lagrange basis on the points, at the points
   void init(int p, int q);
   void eval(double x, double *val, double *der) const;
 };

@@ -68,6 +68,25 @@ void Basis::init(int p_, int q_) {
   if (p % 2 == 0 && p > 0) nodes[p / 2] = 0.5;
   N.assign(q * (p + 1), 0.0); D.assign(q * (p + 1), 0.0);
   for (int k = 0; k < q; ++k) eval(qpts[k], &N[k * (p + 1)], &D[k * (p + 1)]);
+  // collocation derivative: Dc[k][m] = l_m'(x_k) for the Lagrange basis l_m on
+  // the quadrature points (l_m'(x_m) = sum_{j != m} 1 / (x_m - x_j))
+  Dc.assign(q * q, 0.0);
+  for (int k = 0; k < q; ++k)
+    for (int m = 0; m < q; ++m) {
+      if (k == m) {
+        double s = 0.0;
+        for (int j = 0; j < q; ++j)
+          if (j != m) s += 1.0 / (qpts[m] - qpts[j]);
+        Dc[k * q + m] = s;
+      } else {
+        double num = 1.0, den = 1.0;
+        for (int j = 0; j < q; ++j) {
+          if (j != m) den *= qpts[m] - qpts[j];
+          if (j != m && j != k) num *= qpts[k] - qpts[j];
+        }
+        Dc[k * q + m] = num / den;
+      }
+    }
 }
 
 namespace {

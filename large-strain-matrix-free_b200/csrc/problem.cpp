@@ -395,10 +395,9 @@ static lsmf_status validate_params(const ProblemParams &P, int &caching) {
   if (P.caching == "scalar") caching = LSMF_CACHE_SCALAR;
   else if (P.caching == "tensor2") caching = LSMF_CACHE_TENSOR2;
   else if (P.caching == "tensor4") caching = LSMF_CACHE_TENSOR4;
-  else if (P.caching == "scalar_referential" || P.caching == "tensor4_ns") {
-    set_error("MF caching " + P.caching + " is not supported");
-    return LSMF_ERR_UNSUPPORTED;
-  } else { set_error("Unknown caching"); return LSMF_ERR_UNKNOWN_CACHING; }
+  else if (P.caching == "scalar_referential") caching = LSMF_CACHE_SCALAR_REFERENTIAL;
+  else if (P.caching == "tensor4_ns") caching = LSMF_CACHE_TENSOR4_NS;
+  else { set_error("Unknown caching"); return LSMF_ERR_UNKNOWN_CACHING; }
   if (P.formulation != 0 && P.formulation != 1) { set_error("Unknown material formulation"); return LSMF_ERR_PRM; }
   if (P.formulation == 0 && caching != LSMF_CACHE_SCALAR) {
     set_error("formulation 0 requires scalar caching");

@@ -18,7 +18,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblsmf.so")
 
-CACHING = {"scalar": 0, "tensor2": 1, "tensor4": 2}
+CACHING = {"scalar": 0, "tensor2": 1, "tensor4": 2, "scalar_referential": 3, "tensor4_ns": 4}
 GEOM = {"box": 0, "cook": 1}
 MASK_ZERO, MASK_MPI, MASK_RW, MASK_SF, MASK_QD, MASK_DEFAULT = 1, 2, 4, 8, 16, 31
 

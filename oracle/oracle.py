@@ -16,7 +16,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "liborc.so")
 
 GEOM_BOX, GEOM_COOK = 0, 1
-CACHE = {"scalar": 0, "tensor2": 1, "tensor4": 2}
+CACHE = {"scalar": 0, "tensor2": 1, "tensor4": 2, "scalar_referential": 3, "tensor4_ns": 4}
 
 
 def build():

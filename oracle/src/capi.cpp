@@ -119,12 +119,16 @@ void orc_op_cell_apply(void *hh, int cell, const void *in, void *out) {
   else h->od.cell_apply(cell, (const double *)in, (double *)out);
 }
 // which: 0 scalar, 1 second scalar, 2 tensor2 (6/qp), 3 tensor4 (36/qp),
-// 4 jinv_cur (9/qp), 5 jxw_cur; returns the element count
+// 4 inverse Jacobian (9/qp), 5 JxW (both in the frame the variant integrates
+// in), 6 scalar_referential displacement values (3/qp), 7 tensor4_ns (81/qp);
+// returns the element count
 long orc_op_get_table(void *hh, int which, void *out) {
   auto *h = (OpH *)hh;
   auto get = [&](auto &op) -> long {
-    const auto *v = which == 0 ? &op.c_scalar : which == 1 ? &op.c_second : which == 2 ? &op.c_t2
-                  : which == 3 ? &op.c_t4 : which == 4 ? &op.jinv_cur : &op.jxw_cur;
+    const bool ref = op.referential();
+    const auto *v = which == 0 ? &op.c_scalar : (which == 1 || which == 6) ? &op.c_second : which == 2 ? &op.c_t2
+                  : which == 3 ? &op.c_t4 : which == 7 ? &op.c_t4ns
+                  : which == 4 ? (ref ? &op.jinv_ref : &op.jinv_cur) : (ref ? &op.jxw_ref : &op.jxw_cur);
     if (out) std::memcpy(out, v->data(), v->size() * sizeof((*v)[0]));
     return (long)v->size();
   };

@@ -17,13 +17,17 @@ void Operator<Number>::initialize(const Mesh *m, const Basis1D *b, int caching_,
                                   int formulation_) {
   // mf_nh_operator.h:394-443: choose the caching variant, size the tables.
   mesh = m; basis = b; caching = caching_; formulation = formulation_;
-  if (caching < 0 || caching > CACHE_TENSOR4)
+  if (caching < 0 || caching > CACHE_TENSOR4_NS)
     throw std::runtime_error("Unknown caching");  // :441
   if (formulation == 0 && caching != CACHE_SCALAR)
     throw std::runtime_error("formulation 0 needs scalar caching");
   const size_t nqt = (size_t)m->n_cells * nq();
-  c_scalar.clear(); c_second.clear(); c_t2.clear(); c_t4.clear();
+  c_scalar.clear(); c_second.clear(); c_t2.clear(); c_t4.clear(); c_t4ns.clear();
   if (caching == CACHE_SCALAR) c_scalar.resize(nqt);
+  // scalar_referential: c and the displacement at the points (:512-534)
+  if (caching == CACHE_SCALAR_REFERENTIAL) { c_scalar.resize(nqt); c_second.resize(3 * nqt); }
+  // tensor4_ns: dP/dF (81 per point, :563-582)
+  if (caching == CACHE_TENSOR4_NS) c_t4ns.resize(81 * nqt);
   if (caching == CACHE_TENSOR2) { c_scalar.resize(nqt); c_second.resize(nqt); c_t2.resize(6 * nqt); }
   if (caching == CACHE_TENSOR4) { c_t2.resize(6 * nqt); c_t4.resize(36 * nqt); }
   jinv_cur.resize(9 * nqt); jxw_cur.resize(nqt);

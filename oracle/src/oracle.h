@@ -123,7 +123,9 @@ struct Operator {
   // metric of the reference configuration (scalar caching needs both)
   std::vector<Number> jinv_ref, jxw_ref;
   // cache tables, [cell][qp][comp] (mf_nh_operator.h:263-267)
-  std::vector<Number> c_scalar, c_second, c_t2, c_t4;
+  std::vector<Number> c_scalar, c_second, c_t2, c_t4, c_t4ns;
+  // scalar_referential and tensor4_ns work in the reference configuration
+  bool referential() const { return caching == CACHE_SCALAR_REFERENTIAL || caching == CACHE_TENSOR4_NS; }
   std::vector<Number> diag, inv_diag;
   int nq() const { return basis->q * basis->q * basis->q; }
   void initialize(const Mesh *m, const Basis1D *b, int caching, int formulation);

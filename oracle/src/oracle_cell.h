@@ -223,6 +223,18 @@ struct CellOps {
         }
       return;
     }
+    if (caching == CACHE_TENSOR4_NS) {
+      // out_ij = A_ijkl Grad v_kl (double_contract<2,0,3,1>, :1441-1455)
+      const Number *A = &op.c_t4ns[81 * qi];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          Number a = 0;
+          for (int k = 0; k < 3; ++k)
+            for (int l = 0; l < 3; ++l) a += A[((i * 3 + j) * 3 + k) * 3 + l] * g[k][l];
+          Qm[i][j] = a;
+        }
+      return;
+    }
     // scalar caching: F from grad u in the reference configuration
     const double mu = op.mu_cell[cell];
     const Material mat(mu, op.nu, op.formulation);
@@ -298,6 +310,50 @@ struct CellOps {
       }
   }
 
+  // scalar_referential (mf_nh_operator.h:1255-1400): g = Grad v in the
+  // reference configuration; grad_x v = Grad v F^-1, tau and jc as in the
+  // scalar variant, submitted as (jc + grad_x v tau) F^-T (no 1/J: the
+  // integration is over the reference configuration)
+  static void qp_physics_sr(const Operator<Number> &op, int cell, size_t qi, const Number g[3][3],
+                            const Number *Gu_ref, Number Qm[3][3]) {
+    const double mu = op.mu_cell[cell];
+    const Material mat(mu, op.nu, 1);
+    Number F[3][3], Fi[3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) F[i][j] = Gu_ref[i * 3 + j] + (i == j ? Number(1) : Number(0));
+    inv3(F, Fi);
+    Number gx[3][3];
+    for (int d = 0; d < 3; ++d)
+      for (int e = 0; e < 3; ++e) {
+        Number a = 0;
+        for (int f = 0; f < 3; ++f) a += g[d][f] * Fi[f][e];
+        gx[d][e] = a;
+      }
+    const Number c = op.c_scalar[qi];
+    Number tau[3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        Number b = 0;
+        for (int k = 0; k < 3; ++k) b += F[i][k] * F[j][k];
+        tau[i][j] = Number(mu) * b - (i == j ? c : Number(0));
+      }
+    const Number tr = gx[0][0] + gx[1][1] + gx[2][2];
+    Number qd[3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        Number v = Number(2.0) * c * Number(0.5) * (gx[i][j] + gx[j][i]);
+        if (i == j) v += Number(2.0) * Number(mat.lambda) * tr;
+        for (int k = 0; k < 3; ++k) v += gx[i][k] * tau[k][j];
+        qd[i][j] = v;
+      }
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        Number a = 0;
+        for (int k = 0; k < 3; ++k) a += qd[i][k] * Fi[j][k];  // queued * F^-T
+        Qm[i][j] = a;
+      }
+  }
+
   // Cell operator on a local (component-blocked) vector; metric and cache
   // must be available (mf_nh_operator.h:922-1499).
   static void cell_apply_tables(const Tables &t, const Operator<Number> &op, int cell,
@@ -305,14 +361,16 @@ struct CellOps {
     Number G[3][3][NQ], H[3][3][NQ];
     grad(t, in, G);
     Number Gu[3][3][NQ];
-    if (op.caching == CACHE_SCALAR) {
+    const bool need_u = op.caching == CACHE_SCALAR || op.caching == CACHE_SCALAR_REFERENTIAL;
+    if (need_u) {
       Number uloc[3 * NN];
       gather(op, cell, op.u.data(), false, uloc);  // read_dof_values_plain(u)
       grad(t, uloc, Gu);
     }
+    const bool ref = op.referential();
     for (int q = 0; q < NQ; ++q) {
       const size_t qi = (size_t)cell * NQ + q;
-      const Number *Ji = &op.jinv_cur[9 * qi];
+      const Number *Ji = ref ? &op.jinv_ref[9 * qi] : &op.jinv_cur[9 * qi];
       Number g[3][3];
       for (int c = 0; c < 3; ++c)
         for (int d = 0; d < 3; ++d) {
@@ -321,7 +379,7 @@ struct CellOps {
           g[c][d] = a;
         }
       Number gu[9];
-      if (op.caching == CACHE_SCALAR) {
+      if (need_u) {
         const Number *Jr = &op.jinv_ref[9 * qi];
         for (int c = 0; c < 3; ++c)
           for (int d = 0; d < 3; ++d) {
@@ -331,8 +389,9 @@ struct CellOps {
           }
       }
       Number Qm[3][3];
-      qp_physics(op, cell, qi, g, gu, Qm);
-      const Number jxw = op.jxw_cur[qi];
+      if (op.caching == CACHE_SCALAR_REFERENTIAL) qp_physics_sr(op, cell, qi, g, gu, Qm);
+      else qp_physics(op, cell, qi, g, gu, Qm);
+      const Number jxw = ref ? op.jxw_ref[qi] : op.jxw_cur[qi];
       for (int c = 0; c < 3; ++c)
         for (int e = 0; e < 3; ++e) {
           Number a = 0;
@@ -456,6 +515,35 @@ struct CellOps {
         }
         const Number scalar = Number(mat.mu) - Number(2.0) * Number(mat.lambda) * std::log(det_F);
         if (op.caching == CACHE_SCALAR) { op.c_scalar[qi] = scalar; continue; }
+        if (op.caching == CACHE_SCALAR_REFERENTIAL) {
+          // c and the displacement values at the point (phi_reference.begin_values())
+          op.c_scalar[qi] = scalar;
+          const int qx = q % Q, qy = (q / Q) % Q, qz = q / (Q * Q);
+          for (int c = 0; c < 3; ++c) {
+            Number v = 0;
+            for (int kz = 0; kz < N1; ++kz)
+              for (int jy = 0; jy < N1; ++jy)
+                for (int ix = 0; ix < N1; ++ix)
+                  v += Number(t.N[qx][ix] * t.N[qy][jy] * t.N[qz][kz]) * uN[c * NN + (kz * N1 + jy) * N1 + ix];
+            op.c_second[3 * qi + c] = v;
+          }
+          continue;
+        }
+        if (op.caching == CACHE_TENSOR4_NS) {
+          // 2 lambda F^-T (x) F^-T + (mu - 2 lambda ln J) F^-T_il F^-1_jk + mu I_ik I_jl
+          Number Fi[3][3];
+          inv3(F, Fi);
+          const Number lnJ = std::log(det_F);
+          for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+              for (int k = 0; k < 3; ++k)
+                for (int l = 0; l < 3; ++l)
+                  op.c_t4ns[81 * qi + ((i * 3 + j) * 3 + k) * 3 + l] =
+                      Number(2.0) * Number(mat.lambda) * Fi[j][i] * Fi[l][k] +
+                      (Number(mat.mu) - Number(2.0) * Number(mat.lambda) * lnJ) * Fi[l][i] * Fi[j][k] +
+                      (i == k && j == l ? Number(mat.mu) : Number(0));
+          continue;
+        }
         Number tau[6];
         for (int I = 0; I < 6; ++I) {
           const int i = SYM_I[I], j = SYM_J[I];

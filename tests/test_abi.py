@@ -46,10 +46,16 @@ def test_prm_valid():
     assert st == 0, msg
 
 
+@pytest.mark.parametrize("caching", ["scalar", "tensor2", "tensor4", "scalar_referential", "tensor4_ns"])
+def test_prm_every_caching(caching):
+    st, msg = lsmf.prm_validate(prm_text(dict(BASE, **{"MF caching": caching})))
+    assert st == 0, msg
+
+
 @pytest.mark.parametrize("change,status", [
     ({"Solver type": "CG"}, 10),                      # matrix-based path is not part of this library
     ({"Preconditioner type": "amg"}, 10),
-    ({"MF caching": "tensor4_ns"}, 10),
+    ({"MF caching": "tensor4_ns", "Formulation": 0}, 10),   # referential variants are formulation 1
     ({"MF caching": "magic"}, 2),                     # Unknown caching (mf_nh_operator.h:441)
     ({"Formulation": 0}, 10),                         # formulation 0 needs scalar caching
     ({"Dimension": 2}, 10),

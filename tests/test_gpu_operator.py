@@ -44,7 +44,8 @@ def _rel(a, b):
     return np.max(np.abs(a - b)) / np.max(np.abs(b))
 
 
-VARIANTS = [("tensor4", 1), ("tensor2", 1), ("scalar", 1), ("scalar", 0)]
+VARIANTS = [("tensor4", 1), ("tensor2", 1), ("scalar", 1), ("scalar", 0), ("scalar_referential", 1),
+            ("tensor4_ns", 1)]
 
 
 KERNELS = ["bulk1", "bulk2", "bulk3", "plain", "basic"]
@@ -106,7 +107,8 @@ def test_cache_tables_match_oracle(caching, formulation):
     op.set_material(mu, 0.3)
     du = torch.tensor(u, device="cuda")
     op.cache(du)
-    whichs = {"tensor4": [2, 3, 4, 5], "tensor2": [0, 1, 2, 4, 5], "scalar": [0, 4, 5]}[caching]
+    whichs = {"tensor4": [2, 3, 4, 5], "tensor2": [0, 1, 2, 4, 5], "scalar": [0, 4, 5],
+              "scalar_referential": [0, 4, 5, 6], "tensor4_ns": [4, 5, 7]}[caching]
     for w in whichs:
         assert _rel(op.table(w), ref.table(w)) < 1e-13, w
 

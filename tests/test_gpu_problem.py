@@ -70,7 +70,7 @@ def test_newton_gmg_matches_oracle(precision):
     assert np.max(np.abs(u - ref["u"])) <= 1e-7 * np.max(np.abs(ref["u"]))
 
 
-@pytest.mark.parametrize("caching", ["tensor2", "scalar"])
+@pytest.mark.parametrize("caching", ["tensor2", "scalar", "scalar_referential", "tensor4_ns"])
 def test_newton_other_cachings(caching):
     pb = lsmf.Problem(_cook_prm("float", caching=caching, end=0.2, dt=0.2))
     res = pb.run()

@@ -31,7 +31,8 @@ def _problem(caching="tensor4", formulation=1, p=2, coarse=(1, 1, 1), nref=2, se
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-@pytest.mark.parametrize("caching,formulation", [("tensor4", 1), ("tensor2", 1), ("scalar", 1), ("scalar", 0)])
+@pytest.mark.parametrize("caching,formulation", [("tensor4", 1), ("tensor2", 1), ("scalar", 1), ("scalar", 0),
+                                                 ("scalar_referential", 1), ("tensor4_ns", 1)])
 def test_vcycle_matches_oracle(precision, caching, formulation):
     gm, mu, u, dirichlet, (lo, hi), rng = _problem(caching, formulation)
     og = O.GMG(O.GEOM_BOX, (1, 1, 1), 2, lo, hi, 1.0, 2, 3, caching, formulation, precision == "fp32", mu, 0.3,

@@ -48,7 +48,8 @@ def _fields():
 
 
 @pytest.mark.parametrize("name,field,p", _fields(), ids=[f[0] for f in _fields()])
-@pytest.mark.parametrize("formulation,caching", [(0, "scalar"), (1, "scalar"), (1, "tensor2"), (1, "tensor4")])
+@pytest.mark.parametrize("formulation,caching", [(0, "scalar"), (1, "scalar"), (1, "tensor2"), (1, "tensor4"),
+                                                 (1, "scalar_referential"), (1, "tensor4_ns")])
 def test_single_cell_mf_vs_matrix(name, field, p, formulation, caching):
     m = O.Mesh(O.GEOM_BOX, (1, 1, 1), 0, (0, 0, 0), (1, 1, 1), 1.0, p, p + 1)
     # the reference interpolates the field itself as the displacement (for
