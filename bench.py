@@ -37,11 +37,17 @@ METRIC = "Tangent vmult GDoF/s & Newton-step time, FP32-GMG vs FP64, same 1e-8 r
 
 def alg_bytes(variant, S, n_nodes, n_qp, n_cells):
     """Algorithmic bytes per vmult (values counted once, index maps excluded):
-    scalar S(9N + 11Q + 10C), tensor2 S(6N + 18Q), tensor4 S(6N + 52Q)."""
+    scalar S(9N + 11Q + 10C), tensor2 S(6N + 18Q), tensor4 S(6N + 52Q);
+    the referential variants: scalar_referential S(6N + 14Q) (c, the point
+    displacement, metric), tensor4_ns S(6N + 91Q) (dP/dF, metric)."""
     if variant == "tensor4":
         return S * (6 * n_nodes + 52 * n_qp)
     if variant == "tensor2":
         return S * (6 * n_nodes + 18 * n_qp)
+    if variant == "scalar_referential":
+        return S * (6 * n_nodes + 14 * n_qp)
+    if variant == "tensor4_ns":
+        return S * (6 * n_nodes + 91 * n_qp)
     return S * (9 * n_nodes + 11 * n_qp + 10 * n_cells)
 
 
@@ -322,7 +328,7 @@ def run_lsmf(args):
     # per-variant rates (same mesh / inputs)
     variants = {}
     peak, peak_kind = measured_peak()
-    for variant in () if args.no_variants else ("tensor4", "tensor2", "scalar"):
+    for variant in () if args.no_variants else ("tensor4", "tensor2", "scalar", "scalar_referential", "tensor4_ns"):
         for prec in ("fp64", "fp32"):
             if variant == "tensor4" and prec == "fp64":
                 v_op, s_in = op, src64

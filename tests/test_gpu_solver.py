@@ -62,6 +62,30 @@ def test_vcycle_matches_oracle(precision, caching, formulation):
     assert torch.max(torch.abs(d2 - ddst)).item() <= (1e-12 if precision == "fp64" else 1e-5) * np.max(np.abs(got))
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("coarse_chebyshev", [True, False])
+def test_vcycle_large_coarse_level(precision, coarse_chebyshev):
+    # a 6^3-cell coarse level: a high-degree coarse Chebyshev (or the coarse
+    # CG with its Chebyshev preconditioner) over many blocks
+    gm, mu, u, dirichlet, (lo, hi), rng = _problem("tensor4", 1, coarse=(6, 6, 6), nref=1)
+    og = O.GMG(O.GEOM_BOX, (6, 6, 6), 1, lo, hi, 1.0, 2, 3, "tensor4", 1, precision == "fp32", mu, 0.3,
+               dirichlet, u, coarse_chebyshev=coarse_chebyshev)
+    g = lsmf.GMG(gm, "tensor4", 1, precision, coarse_chebyshev=coarse_chebyshev)
+    g.set_material(mu, 0.3)
+    du = torch.tensor(u, device="cuda")
+    g.setup(du)
+    a, b = g.level_info(0), og.level_info(0)
+    assert a[2] == b[2] and (a[2] > 20 or not coarse_chebyshev), (a, b)
+    src = rng.uniform(-1, 1, u.size)
+    src[gm.constraint_mask() == 1] = 0
+    dsrc = torch.tensor(src, device="cuda")
+    ddst = torch.empty_like(dsrc)
+    g.vmult(ddst, dsrc)
+    got, want = ddst.cpu().numpy(), og.vmult(src)
+    tol = 1e-10 if precision == "fp64" else 1e-4
+    assert np.max(np.abs(got - want)) <= tol * np.max(np.abs(want))
+
+
 def test_vcycle_cook_geometry():
     gm, mu, u, dirichlet, (lo, hi), rng = _problem("tensor4", 1, coarse=(2, 2, 1), nref=1, geometry="cook")
     og = O.GMG(O.GEOM_COOK, (2, 2, 1), 1, lo, hi, 1.0, 2, 3, "tensor4", 1, False, mu, 0.3, dirichlet, u)
