@@ -80,12 +80,11 @@ lsmf_status estimate_eigenvalues(lsmf_gmg *g, int l, int max_it, double &emin, d
   cudaStream_t st = g->stream;
   T *x = (T *)g->eig_vecs.ptr, *gg = x + n, *h = gg + n, *d = h + n;
   const T *invd = (const T *)op->d_inv_diag.ptr;
-  std::vector<T> rhs(n);
-  double mean = 0;
-  for (size_t i = 0; i < n; ++i) mean += (double)(i % 11);
-  mean /= (double)n;
-  for (size_t i = 0; i < n; ++i) rhs[i] = T(mean - (double)(i % 11));  // g = A 0 - b
-  LSMF_CUDA(cudaMemcpyAsync(gg, rhs.data(), n * sizeof(T), cudaMemcpyHostToDevice, st));
+  // start vector (i mod 11) - mean, made on the device; the mean of the
+  // integers i mod 11 is exact in closed form (the sum is below 2^53)
+  const size_t q11 = n / 11, r11 = n % 11;
+  const double mean = (double)(55 * q11 + r11 * (r11 - 1) / 2) / (double)n;
+  LSMF_TRY(eig_start_async<T>(gg, n, mean, st));  // g = A 0 - b
   LSMF_CUDA(cudaMemsetAsync(x, 0, n * sizeof(T), st));
   double *sc = g->sc.ptr, *part = g->partial.ptr;
   const bool fp32 = sizeof(T) == 4;
@@ -118,25 +117,66 @@ lsmf_status estimate_eigenvalues(lsmf_gmg *g, int l, int max_it, double &emin, d
     if (g->eig_hist.n < need) LSMF_TRY(g->eig_hist.alloc(need));
     const size_t stride = need / 3;
     double *ha = g->eig_hist.ptr, *hb = ha + stride, *hr = hb + stride;
-    int k = 0;
-    bool done = false;
-    std::vector<double> A(8), Bt(8), Rs(8);
-    double prev_beta = 0, prev_alpha = 0;
-    while (!done && k < max_it) {
-      const int batch = std::min(8, max_it - k);
-      for (int j = 0; j < batch; ++j, ++k) {
+    // one batch of iterations k0 + j, j < batch; with kbase the history
+    // index is *kbase + j and the batch is the same launch sequence every
+    // time (parity of k0 even), so it can be captured once and replayed
+    auto batch_launch = [&](int k0, int batch, const int *kbase) -> lsmf_status {
+      for (int j = 0; j < batch; ++j) {
+        const int k = k0 + j;
         const int gh = SC_GH0 + (k & 1), ghn = SC_GH0 + ((k + 1) & 1);
+        const int kh = kbase ? j : k;
         LSMF_TRY(launch_apply(op, h, d, LSMF_MASK_DEFAULT, false));
         LSMF_TRY(dot_async(d, h, fp32, n, part, sc, SC_DH, st));
-        LSMF_TRY(eig_update_async<T>(gg, h, n, sc, gh, ha, hr, k, part, st));
+        LSMF_TRY(eig_update_async<T>(gg, h, n, sc, gh, ha, hr, kh, kbase, part, st));
         LSMF_TRY(jacobi_async<T>(h, invd, gg, 1.0, n, st));
         LSMF_TRY(dot_async(gg, h, fp32, n, part, sc, ghn, st));
-        LSMF_TRY(eig_dir_async<T>(d, h, n, sc, ghn, gh, hb, k, st));
+        LSMF_TRY(eig_dir_async<T>(d, h, n, sc, ghn, gh, hb, kh, kbase, st));
       }
-      LSMF_CUDA(cudaMemcpyAsync(A.data(), ha + (k - batch), batch * sizeof(double), cudaMemcpyDeviceToHost, st));
-      LSMF_CUDA(cudaMemcpyAsync(Bt.data(), hb + (k - batch), batch * sizeof(double), cudaMemcpyDeviceToHost, st));
-      LSMF_CUDA(cudaMemcpyAsync(Rs.data(), hr + (k - batch), batch * sizeof(double), cudaMemcpyDeviceToHost, st));
-      LSMF_CUDA(cudaStreamSynchronize(st));
+      if (kbase) LSMF_TRY(eig_advance_async(const_cast<int *>(kbase), batch, st));
+      return LSMF_OK;
+    };
+    // long estimates (the coarse solver's, up to n iterations) replay a
+    // captured batch: one graph launch instead of ~70 kernel launches
+    cudaGraphExec_t bexec = nullptr;
+    if (g->use_graph && max_it >= 64) {
+      if (g->eig_kbase.n < 1) LSMF_TRY(g->eig_kbase.alloc(1));
+      LSMF_CUDA(cudaMemsetAsync(g->eig_kbase.ptr, 0, sizeof(int), st));
+      if (!g->cap_stream) LSMF_CUDA(cudaStreamCreateWithFlags(&g->cap_stream, cudaStreamNonBlocking));
+      const cudaStream_t user = st;
+      lsmf_gmg_set_stream(g, g->cap_stream);
+      st = g->cap_stream;
+      LSMF_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+      const lsmf_status s = batch_launch(0, 8, g->eig_kbase.ptr);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(st, &graph);
+      lsmf_gmg_set_stream(g, user);
+      st = user;
+      if (s != LSMF_OK) { if (graph) cudaGraphDestroy(graph); return s; }
+      if (e != cudaSuccess) { set_error(std::string("eigenvalue CG capture: ") + cudaGetErrorString(e)); return LSMF_ERR_CUDA; }
+      const cudaError_t ei = cudaGraphInstantiate(&bexec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ei != cudaSuccess) { set_error(std::string("eigenvalue CG graph: ") + cudaGetErrorString(ei)); return LSMF_ERR_CUDA; }
+    }
+    int k = 0;
+    bool done = false;
+    lsmf_status status = LSMF_OK;
+    std::vector<double> A(8), Bt(8), Rs(8);
+    double prev_beta = 0, prev_alpha = 0;
+    while (!done && k < max_it && status == LSMF_OK) {
+      const int batch = std::min(8, max_it - k);
+      if (bexec && batch == 8) {
+        // the replayed batch writes history k .. k + 7 (its base is k)
+        const cudaError_t e = cudaGraphLaunch(bexec, st);
+        if (e != cudaSuccess) { set_error(std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); status = LSMF_ERR_CUDA; break; }
+      } else if ((status = batch_launch(k, batch, nullptr)) != LSMF_OK) {
+        break;
+      }
+      k += batch;
+      cudaError_t e = cudaMemcpyAsync(A.data(), ha + (k - batch), batch * sizeof(double), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(Bt.data(), hb + (k - batch), batch * sizeof(double), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(Rs.data(), hr + (k - batch), batch * sizeof(double), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) { set_error(std::string("eigenvalue CG history: ") + cudaGetErrorString(e)); status = LSMF_ERR_CUDA; break; }
       for (int j = 0; j < batch && !done; ++j) {
         ++its;
         const double alpha = A[j];
@@ -151,6 +191,8 @@ lsmf_status estimate_eigenvalues(lsmf_gmg *g, int l, int max_it, double &emin, d
         prev_alpha = alpha;
       }
     }
+    if (bexec) cudaGraphExecDestroy(bexec);
+    if (status != LSMF_OK) return status;
   }
   emin = emax = 1.0;
   if (!dT.empty()) {

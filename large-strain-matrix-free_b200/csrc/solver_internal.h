@@ -18,12 +18,18 @@ lsmf_status cg_update_async(double *x, double *g, const double *d, const double 
                             double *partial, cudaStream_t st);
 lsmf_status cg_dir_async(double *d, const double *h, size_t n, const double *sc, int gh_new, int gh_old, bool first,
                          cudaStream_t st);
+// one eigenvalue-CG step's updates; the history index is k, plus *kbase when
+// kbase is given (a replayed batch whose base advances on the device)
 template <typename T>
 lsmf_status eig_update_async(T *g, const T *h, size_t n, double *sc, int gh_slot, double *hist_alpha, double *hist_res2,
-                             int k, double *partial, cudaStream_t st);
+                             int k, const int *kbase, double *partial, cudaStream_t st);
 template <typename T>
 lsmf_status eig_dir_async(T *d, const T *h, size_t n, const double *sc, int gh_new, int gh_old, double *hist_beta,
-                          int k, cudaStream_t st);
+                          int k, const int *kbase, cudaStream_t st);
+lsmf_status eig_advance_async(int *kbase, int by, cudaStream_t st);
+// g = A 0 - b for the start vector b_i = (i mod 11) - mean
+template <typename T>
+lsmf_status eig_start_async(T *g, size_t n, double mean, cudaStream_t st);
 template <typename T>
 lsmf_status neg_residual_async(T *g, const T *ax, const T *b, size_t n, cudaStream_t st);
 template <typename T>
@@ -93,6 +99,7 @@ struct lsmf_gmg {
   lsmf::DevBuf<double> sc, partial;
   lsmf::DevBuf<char> eig_vecs;  // scratch for the eigenvalue CG (4 level vectors)
   lsmf::DevBuf<double> eig_hist; // alpha / beta / residual history of the eigenvalue CG
+  lsmf::DevBuf<int> eig_kbase;   // history base of the replayed eigenvalue-CG batches
   cudaStream_t stream = 0;
   bool ready = false;
   // the V-cycle replayed as one CUDA graph (captured after each set-up)

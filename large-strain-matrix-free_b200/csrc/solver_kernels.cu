@@ -33,8 +33,8 @@ __global__ void dot_partial_kernel(const A *a, const B *b, size_t n, double *par
   }
 }
 
-// sums partial[0..n) in a fixed order into *out
-__global__ void reduce_final_kernel(const double *partial, int n, double *out) {
+// sums partial[0..n) in a fixed order into out[*koff] (out[0] without koff)
+__global__ void reduce_final_kernel(const double *partial, int n, double *out, const int *koff = nullptr) {
   __shared__ double sh[32];
   double s = 0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) s += partial[i];
@@ -44,7 +44,7 @@ __global__ void reduce_final_kernel(const double *partial, int n, double *out) {
   if (threadIdx.x < 32) {
     s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (threadIdx.x == 0) *out = s;
+    if (threadIdx.x == 0) out[koff ? *koff : 0] = s;
   }
 }
 
@@ -82,10 +82,10 @@ __global__ void cg_dir_kernel(double *d, const double *h, size_t n, const double
 // partial sums of g.g; alpha recorded in hist_alpha[k]
 template <typename T>
 __global__ void eig_update_kernel(T *g, const T *h, size_t n, const double *sc, int gh_slot, double *hist_alpha,
-                                  int k, double *partial) {
+                                  int k, const int *kbase, double *partial) {
   __shared__ double sh[RED_THREADS / 32];
   const double alpha = sc[gh_slot] / sc[SC_DH];
-  if (blockIdx.x == 0 && threadIdx.x == 0) hist_alpha[k] = alpha;
+  if (blockIdx.x == 0 && threadIdx.x == 0) hist_alpha[(kbase ? *kbase : 0) + k] = alpha;
   double s = 0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const double gi = (double)g[i] + alpha * (double)h[i];
@@ -105,11 +105,21 @@ __global__ void eig_update_kernel(T *g, const T *h, size_t n, const double *sc, 
 // d = beta d - h with beta = sc[gh_new] / sc[gh_old], recorded in hist_beta[k]
 template <typename T>
 __global__ void eig_dir_kernel(T *d, const T *h, size_t n, const double *sc, int gh_new, int gh_old, double *hist_beta,
-                               int k) {
+                               int k, const int *kbase) {
   const double beta = sc[gh_new] / sc[gh_old];
-  if (blockIdx.x == 0 && threadIdx.x == 0) hist_beta[k] = beta;
+  if (blockIdx.x == 0 && threadIdx.x == 0) hist_beta[(kbase ? *kbase : 0) + k] = beta;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     d[i] = T(beta * (double)d[i] - (double)h[i]);
+}
+
+// history base of a replayed batch of eigenvalue-CG iterations
+__global__ void eig_advance_kernel(int *kbase, int by) { *kbase += by; }
+
+// eigenvalue-CG start: g = A 0 - b with b_i = (i mod 11) - mean
+template <typename T>
+__global__ void eig_start_kernel(T *g, size_t n, double mean) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    g[i] = T(mean - (double)(i % 11));
 }
 
 template <typename T>
@@ -474,31 +484,54 @@ lsmf_status cg_update_async(double *x, double *g, const double *d, const double 
   return LSMF_OK;
 }
 
+static void eig_index_final(const double *partial, int gr, double *out, const int *kbase, cudaStream_t st) {
+  reduce_final_kernel<<<1, 1024, 0, st>>>(partial, gr, out, kbase);
+}
+
 template <typename T>
 lsmf_status eig_update_async(T *g, const T *h, size_t n, double *sc, int gh_slot, double *hist_alpha, double *hist_res2,
-                             int k, double *partial, cudaStream_t st) {
+                             int k, const int *kbase, double *partial, cudaStream_t st) {
   const int gr = reduce_blocks();
-  eig_update_kernel<T><<<gr, RED_THREADS, 0, st>>>(g, h, n, sc, gh_slot, hist_alpha, k, partial);
-  reduce_final_kernel<<<1, 1024, 0, st>>>(partial, gr, hist_res2 + k);
+  eig_update_kernel<T><<<gr, RED_THREADS, 0, st>>>(g, h, n, sc, gh_slot, hist_alpha, k, kbase, partial);
+  if (kbase) {
+    eig_index_final(partial, gr, hist_res2 + k, kbase, st);
+  } else {
+    reduce_final_kernel<<<1, 1024, 0, st>>>(partial, gr, hist_res2 + k);
+  }
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
 }
 template lsmf_status eig_update_async<float>(float *, const float *, size_t, double *, int, double *, double *, int,
-                                             double *, cudaStream_t);
+                                             const int *, double *, cudaStream_t);
 template lsmf_status eig_update_async<double>(double *, const double *, size_t, double *, int, double *, double *, int,
-                                              double *, cudaStream_t);
+                                              const int *, double *, cudaStream_t);
 
 template <typename T>
 lsmf_status eig_dir_async(T *d, const T *h, size_t n, const double *sc, int gh_new, int gh_old, double *hist_beta,
-                          int k, cudaStream_t st) {
-  eig_dir_kernel<T><<<vec_grid(n), 256, 0, st>>>(d, h, n, sc, gh_new, gh_old, hist_beta, k);
+                          int k, const int *kbase, cudaStream_t st) {
+  eig_dir_kernel<T><<<vec_grid(n), 256, 0, st>>>(d, h, n, sc, gh_new, gh_old, hist_beta, k, kbase);
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
 }
 template lsmf_status eig_dir_async<float>(float *, const float *, size_t, const double *, int, int, double *, int,
-                                          cudaStream_t);
+                                          const int *, cudaStream_t);
 template lsmf_status eig_dir_async<double>(double *, const double *, size_t, const double *, int, int, double *, int,
-                                           cudaStream_t);
+                                           const int *, cudaStream_t);
+
+lsmf_status eig_advance_async(int *kbase, int by, cudaStream_t st) {
+  eig_advance_kernel<<<1, 1, 0, st>>>(kbase, by);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+
+template <typename T>
+lsmf_status eig_start_async(T *g, size_t n, double mean, cudaStream_t st) {
+  eig_start_kernel<T><<<vec_grid(n), 256, 0, st>>>(g, n, mean);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+template lsmf_status eig_start_async<float>(float *, size_t, double, cudaStream_t);
+template lsmf_status eig_start_async<double>(double *, size_t, double, cudaStream_t);
 
 lsmf_status cg_dir_async(double *d, const double *h, size_t n, const double *sc, int gh_new, int gh_old, bool first,
                          cudaStream_t st) {
