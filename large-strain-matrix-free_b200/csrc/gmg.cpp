@@ -80,6 +80,7 @@ lsmf_status estimate_eigenvalues(lsmf_gmg *g, int l, int max_it, double &emin, d
   cudaStream_t st = g->stream;
   T *x = (T *)g->eig_vecs.ptr, *gg = x + n, *h = gg + n, *d = h + n;
   const T *invd = (const T *)op->d_inv_diag.ptr;
+  const uint8_t *cm = op->L().d_cmask.ptr;
   // start vector (i mod 11) - mean, made on the device; the mean of the
   // integers i mod 11 is exact in closed form (the sum is below 2^53)
   const size_t q11 = n / 11, r11 = n % 11;
@@ -105,6 +106,7 @@ lsmf_status estimate_eigenvalues(lsmf_gmg *g, int l, int max_it, double &emin, d
     LSMF_CUDA(cudaMemsetAsync(d, 0, n * sizeof(T), st));
     LSMF_TRY(dir_async<T>(d, h, 0.0, n, st));  // d = -h
     LSMF_TRY(dot_async(gg, h, fp32, n, part, sc, SC_GH0, st));
+    LSMF_CUDA(cudaMemsetAsync(h, 0, n * sizeof(T), st));  // the cell loop accumulates into h
     // CG iterations run in batches of 8 with device-resident scalars; the
     // alpha / beta / residual history is read once per batch and the Lanczos
     // matrix is cut at the first iteration that meets the tolerance, so the
@@ -121,16 +123,16 @@ lsmf_status estimate_eigenvalues(lsmf_gmg *g, int l, int max_it, double &emin, d
     // index is *kbase + j and the batch is the same launch sequence every
     // time (parity of k0 even), so it can be captured once and replayed
     auto batch_launch = [&](int k0, int batch, const int *kbase) -> lsmf_status {
+      // per iteration: cell loop into h (zero on entry), identity rows + d.h,
+      // g update + Jacobi + g.g and g.h, direction update that clears h
       for (int j = 0; j < batch; ++j) {
         const int k = k0 + j;
         const int gh = SC_GH0 + (k & 1), ghn = SC_GH0 + ((k + 1) & 1);
         const int kh = kbase ? j : k;
-        LSMF_TRY(launch_apply(op, h, d, LSMF_MASK_DEFAULT, false));
-        LSMF_TRY(dot_async(d, h, fp32, n, part, sc, SC_DH, st));
-        LSMF_TRY(eig_update_async<T>(gg, h, n, sc, gh, ha, hr, kh, kbase, part, st));
-        LSMF_TRY(jacobi_async<T>(h, invd, gg, 1.0, n, st));
-        LSMF_TRY(dot_async(gg, h, fp32, n, part, sc, ghn, st));
-        LSMF_TRY(eig_dir_async<T>(d, h, n, sc, ghn, gh, hb, kh, kbase, st));
+        LSMF_TRY(launch_apply_cells(op, h, d));
+        LSMF_TRY(eig_dh_async<T>(d, h, cm, n, part, sc, st));
+        LSMF_TRY(eig_update_precond_async<T>(gg, h, invd, n, sc, gh, ghn, ha, hr, kh, kbase, part, st));
+        LSMF_TRY(eig_dir_clear_async<T>(d, h, n, sc, ghn, gh, hb, kh, kbase, st));
       }
       if (kbase) LSMF_TRY(eig_advance_async(const_cast<int *>(kbase), batch, st));
       return LSMF_OK;
@@ -407,7 +409,7 @@ lsmf_status lsmf_gmg_create(lsmf_mesh *m, const lsmf_gmg_desc *desc, lsmf_gmg **
       break;
   }
   if (s == LSMF_OK) s = g->sc.alloc(SC_N);
-  if (s == LSMF_OK) s = g->partial.alloc(reduce_blocks());
+  if (s == LSMF_OK) s = g->partial.alloc(2 * (size_t)reduce_blocks());  // two partial-sum arrays
   if (s == LSMF_OK) s = g->eig_vecs.alloc(4 * nmax);
   if (s != LSMF_OK) { delete g; return s; }
   g->mu_fine.assign(m->levels.back()->n_cells, 1.0);

@@ -18,15 +18,22 @@ lsmf_status cg_update_async(double *x, double *g, const double *d, const double 
                             double *partial, cudaStream_t st);
 lsmf_status cg_dir_async(double *d, const double *h, size_t n, const double *sc, int gh_new, int gh_old, bool first,
                          cudaStream_t st);
-// one eigenvalue-CG step's updates; the history index is k, plus *kbase when
-// kbase is given (a replayed batch whose base advances on the device)
-template <typename T>
-lsmf_status eig_update_async(T *g, const T *h, size_t n, double *sc, int gh_slot, double *hist_alpha, double *hist_res2,
-                             int k, const int *kbase, double *partial, cudaStream_t st);
-template <typename T>
-lsmf_status eig_dir_async(T *d, const T *h, size_t n, const double *sc, int gh_new, int gh_old, double *hist_beta,
-                          int k, const int *kbase, cudaStream_t st);
 lsmf_status eig_advance_async(int *kbase, int by, cudaStream_t st);
+// fused eigenvalue-CG step (h holds the cell part of A d on entry):
+//   eig_dh: identity rows h_c += d_c, sc[DH] = d.h
+//   eig_update_precond: alpha = sc[gh]/sc[DH] (hist), g += alpha h,
+//     h = D^-1 g, hist_res2 = g.g, sc[gh_new] = g.h
+//   eig_dir_clear: beta = sc[gh_new]/sc[gh] (hist), d = beta d - h, h = 0
+// (partial needs 2 * reduce_blocks() doubles)
+template <typename T>
+lsmf_status eig_dh_async(const T *d, T *h, const uint8_t *cmask, size_t n, double *partial, double *sc, cudaStream_t st);
+template <typename T>
+lsmf_status eig_update_precond_async(T *g, T *h, const T *invd, size_t n, double *sc, int gh_slot, int gh_new,
+                                     double *hist_alpha, double *hist_res2, int k, const int *kbase, double *partial,
+                                     cudaStream_t st);
+template <typename T>
+lsmf_status eig_dir_clear_async(T *d, T *h, size_t n, const double *sc, int gh_new, int gh_old, double *hist_beta, int k,
+                                const int *kbase, cudaStream_t st);
 // g = A 0 - b for the start vector b_i = (i mod 11) - mean
 template <typename T>
 lsmf_status eig_start_async(T *g, size_t n, double mean, cudaStream_t st);

@@ -78,40 +78,6 @@ __global__ void cg_dir_kernel(double *d, const double *h, size_t n, const double
     d[i] = beta * d[i] - h[i];
 }
 
-// eigenvalue CG (level precision): alpha = sc[gh] / sc[DH]; g += alpha h;
-// partial sums of g.g; alpha recorded in hist_alpha[k]
-template <typename T>
-__global__ void eig_update_kernel(T *g, const T *h, size_t n, const double *sc, int gh_slot, double *hist_alpha,
-                                  int k, const int *kbase, double *partial) {
-  __shared__ double sh[RED_THREADS / 32];
-  const double alpha = sc[gh_slot] / sc[SC_DH];
-  if (blockIdx.x == 0 && threadIdx.x == 0) hist_alpha[(kbase ? *kbase : 0) + k] = alpha;
-  double s = 0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const double gi = (double)g[i] + alpha * (double)h[i];
-    g[i] = T(gi);
-    s += (double)g[i] * (double)g[i];
-  }
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (threadIdx.x == 0) partial[blockIdx.x] = s;
-  }
-}
-
-// d = beta d - h with beta = sc[gh_new] / sc[gh_old], recorded in hist_beta[k]
-template <typename T>
-__global__ void eig_dir_kernel(T *d, const T *h, size_t n, const double *sc, int gh_new, int gh_old, double *hist_beta,
-                               int k, const int *kbase) {
-  const double beta = sc[gh_new] / sc[gh_old];
-  if (blockIdx.x == 0 && threadIdx.x == 0) hist_beta[(kbase ? *kbase : 0) + k] = beta;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    d[i] = T(beta * (double)d[i] - (double)h[i]);
-}
-
 // history base of a replayed batch of eigenvalue-CG iterations
 __global__ void eig_advance_kernel(int *kbase, int by) { *kbase += by; }
 
@@ -120,6 +86,87 @@ template <typename T>
 __global__ void eig_start_kernel(T *g, size_t n, double mean) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     g[i] = T(mean - (double)(i % 11));
+}
+
+// block sum of s into partial[blockIdx.x] (same pattern as dot_partial_kernel)
+__device__ __forceinline__ void block_partial(double s, double *partial) {
+  __shared__ double sh[RED_THREADS / 32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  }
+  __syncthreads();  // sh may be reused by a second call
+}
+
+template <typename T>
+__global__ void eig_dh_kernel(const T *d, T *h, const uint8_t *cmask, size_t n, double *partial) {
+  double s = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    T hi = h[i];
+    if (cmask[i]) {
+      hi = hi + d[i];  // constrained row: identity
+      h[i] = hi;
+    }
+    s += (double)d[i] * (double)hi;
+  }
+  block_partial(s, partial);
+}
+
+template <typename T>
+__global__ void eig_update_precond_kernel(T *g, T *h, const T *invd, size_t n, const double *sc, int gh_slot,
+                                          double *hist_alpha, int k, const int *kbase, double *partial_gg,
+                                          double *partial_gh) {
+  const double alpha = sc[gh_slot] / sc[SC_DH];
+  if (blockIdx.x == 0 && threadIdx.x == 0) hist_alpha[(kbase ? *kbase : 0) + k] = alpha;
+  double s1 = 0, s2 = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const T gi = T((double)g[i] + alpha * (double)h[i]);
+    g[i] = gi;
+    s1 += (double)gi * (double)gi;
+    const T hi = T(1) * invd[i] * gi;  // Jacobi, omega = 1
+    h[i] = hi;
+    s2 += (double)gi * (double)hi;
+  }
+  block_partial(s1, partial_gg);
+  block_partial(s2, partial_gh);
+}
+
+// two fixed-order sums: p1 -> out1[*koff1], p2 -> *out2
+__global__ void reduce2_final_kernel(const double *p1, const double *p2, int n, double *out1, const int *koff1,
+                                     double *out2) {
+  __shared__ double sh[32];
+  for (int pass = 0; pass < 2; ++pass) {
+    const double *p = pass == 0 ? p1 : p2;
+    double s = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += p[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      if (threadIdx.x == 0) {
+        if (pass == 0) out1[koff1 ? *koff1 : 0] = s;
+        else *out2 = s;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+__global__ void eig_dir_clear_kernel(T *d, T *h, size_t n, const double *sc, int gh_new, int gh_old, double *hist_beta,
+                                     int k, const int *kbase) {
+  const double beta = sc[gh_new] / sc[gh_old];
+  if (blockIdx.x == 0 && threadIdx.x == 0) hist_beta[(kbase ? *kbase : 0) + k] = beta;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    d[i] = T(beta * (double)d[i] - (double)h[i]);
+    h[i] = T(0);
+  }
 }
 
 template <typename T>
@@ -484,39 +531,47 @@ lsmf_status cg_update_async(double *x, double *g, const double *d, const double 
   return LSMF_OK;
 }
 
-static void eig_index_final(const double *partial, int gr, double *out, const int *kbase, cudaStream_t st) {
-  reduce_final_kernel<<<1, 1024, 0, st>>>(partial, gr, out, kbase);
-}
-
 template <typename T>
-lsmf_status eig_update_async(T *g, const T *h, size_t n, double *sc, int gh_slot, double *hist_alpha, double *hist_res2,
-                             int k, const int *kbase, double *partial, cudaStream_t st) {
+lsmf_status eig_dh_async(const T *d, T *h, const uint8_t *cmask, size_t n, double *partial, double *sc,
+                         cudaStream_t st) {
   const int gr = reduce_blocks();
-  eig_update_kernel<T><<<gr, RED_THREADS, 0, st>>>(g, h, n, sc, gh_slot, hist_alpha, k, kbase, partial);
-  if (kbase) {
-    eig_index_final(partial, gr, hist_res2 + k, kbase, st);
-  } else {
-    reduce_final_kernel<<<1, 1024, 0, st>>>(partial, gr, hist_res2 + k);
-  }
+  eig_dh_kernel<T><<<gr, RED_THREADS, 0, st>>>(d, h, cmask, n, partial);
+  reduce_final_kernel<<<1, 1024, 0, st>>>(partial, gr, sc + SC_DH);
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
 }
-template lsmf_status eig_update_async<float>(float *, const float *, size_t, double *, int, double *, double *, int,
-                                             const int *, double *, cudaStream_t);
-template lsmf_status eig_update_async<double>(double *, const double *, size_t, double *, int, double *, double *, int,
-                                              const int *, double *, cudaStream_t);
+template lsmf_status eig_dh_async<float>(const float *, float *, const uint8_t *, size_t, double *, double *,
+                                         cudaStream_t);
+template lsmf_status eig_dh_async<double>(const double *, double *, const uint8_t *, size_t, double *, double *,
+                                          cudaStream_t);
 
 template <typename T>
-lsmf_status eig_dir_async(T *d, const T *h, size_t n, const double *sc, int gh_new, int gh_old, double *hist_beta,
-                          int k, const int *kbase, cudaStream_t st) {
-  eig_dir_kernel<T><<<vec_grid(n), 256, 0, st>>>(d, h, n, sc, gh_new, gh_old, hist_beta, k, kbase);
+lsmf_status eig_update_precond_async(T *g, T *h, const T *invd, size_t n, double *sc, int gh_slot, int gh_new,
+                                     double *hist_alpha, double *hist_res2, int k, const int *kbase, double *partial,
+                                     cudaStream_t st) {
+  const int gr = reduce_blocks();
+  eig_update_precond_kernel<T><<<gr, RED_THREADS, 0, st>>>(g, h, invd, n, sc, gh_slot, hist_alpha, k, kbase, partial,
+                                                           partial + gr);
+  reduce2_final_kernel<<<1, 1024, 0, st>>>(partial, partial + gr, gr, hist_res2 + k, kbase, sc + gh_new);
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
 }
-template lsmf_status eig_dir_async<float>(float *, const float *, size_t, const double *, int, int, double *, int,
-                                          const int *, cudaStream_t);
-template lsmf_status eig_dir_async<double>(double *, const double *, size_t, const double *, int, int, double *, int,
-                                           const int *, cudaStream_t);
+template lsmf_status eig_update_precond_async<float>(float *, float *, const float *, size_t, double *, int, int,
+                                                     double *, double *, int, const int *, double *, cudaStream_t);
+template lsmf_status eig_update_precond_async<double>(double *, double *, const double *, size_t, double *, int, int,
+                                                      double *, double *, int, const int *, double *, cudaStream_t);
+
+template <typename T>
+lsmf_status eig_dir_clear_async(T *d, T *h, size_t n, const double *sc, int gh_new, int gh_old, double *hist_beta, int k,
+                                const int *kbase, cudaStream_t st) {
+  eig_dir_clear_kernel<T><<<vec_grid(n), 256, 0, st>>>(d, h, n, sc, gh_new, gh_old, hist_beta, k, kbase);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+template lsmf_status eig_dir_clear_async<float>(float *, float *, size_t, const double *, int, int, double *, int,
+                                                const int *, cudaStream_t);
+template lsmf_status eig_dir_clear_async<double>(double *, double *, size_t, const double *, int, int, double *, int,
+                                                 const int *, cudaStream_t);
 
 lsmf_status eig_advance_async(int *kbase, int by, cudaStream_t st) {
   eig_advance_kernel<<<1, 1, 0, st>>>(kbase, by);
