@@ -249,6 +249,162 @@ def newton_step_times(cells=15, refinements=2, repeats=3):
     return out
 
 
+def adjoint_prm(cells=8, refinements=2):
+    """Adjoint workload: unit cube, cells^3 coarse cells refined twice (32^3
+    Q2 cells, 823,875 DoFs), bottom clamped, traction (0.02 t, 0, -0.05 t) on
+    the top face, one load step solved to a tight Newton tolerance (relative
+    1e-14, no absolute stop) with FP32 GMG levels and an FP64 outer CG to
+    1e-12."""
+    keys = [("Finite element system", [("Polynomial degree", 2), ("Quadrature order", 3)]),
+            ("Geometry", [("Dimension", 3), ("Type", "Box"), ("Box cells", "%d, %d, %d" % ((cells,) * 3)),
+                          ("Global refinement", refinements)]),
+            ("Material properties", [("Shear modulus", 1.0), ("Poisson's ratio", 0.3), ("Formulation", 1)]),
+            ("Linear solver", [("Solver type", "MF_CG"), ("Residual", 1e-12), ("Preconditioner type", "gmg"),
+                               ("MF caching", "tensor4"), ("MF level precision", "float")]),
+            ("Nonlinear solver", [("Max iterations Newton-Raphson", 25), ("Tolerance force", 1e-14),
+                                  ("Tolerance displacement", 1e-14), ("Absolute tolerance force", 1e-17),
+                                  ("Absolute tolerance displacement", 1e-17)]),
+            ("Boundary conditions", [("Dirichlet IDs and expressions", "4:0,0,0"),
+                                     ("Dirichlet IDs and component mask", "4:true,true,true"),
+                                     ("Neumann IDs and expressions", "5:0.02*t,0,-0.05*t")]),
+            ("Time", [("End time", 1), ("Time step size", 1)])]
+    out = []
+    for sub, kv in keys:
+        out.append("subsection %s" % sub)
+        out += ["  set %s = %s" % (k, v) for k, v in kv]
+        out.append("end")
+    return "\n".join(out) + "\n"
+
+
+def adjoint_times(seed=4321, fd_directions=2, h=1e-4):
+    """Adjoint gradient of J = 1/2 ||u - u_target||^2 on the top face with
+    respect to log mu per cell (log mu ~ N(0, 0.3^2), seeded): device-synced
+    times of the forward solve and the backward (adjoint) pass, and the
+    relative difference to central finite differences (step 1e-4, truncation
+    error ~1e-8) along seeded unit directions."""
+    import torch
+    import lsmf
+    pb = lsmf.Problem(adjoint_prm())
+    rng = np.random.default_rng(seed)
+    theta = rng.normal(0.0, 0.3, pb.n_cells)
+    target = rng.uniform(-1e-3, 1e-3, pb.n_dofs)
+    pb.adjoint_forward(theta, target, 5)  # warm-up
+    pb.adjoint_backward()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pb.adjoint_forward(theta, target, 5)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    grad = pb.adjoint_backward()
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    err = 0.0
+    for _ in range(fd_directions):
+        v = rng.normal(size=pb.n_cells)
+        v /= np.linalg.norm(v)
+        fd = (pb.adjoint_forward(theta + h * v, target, 5) - pb.adjoint_forward(theta - h * v, target, 5)) / (2 * h)
+        err = max(err, abs(fd - grad @ v) / max(abs(fd), 1e-300))
+    return {"workload": "32^3 Q2 unit cube (823,875 DoFs), log mu ~ N(0, 0.3^2) per cell, top-face objective",
+            "n_dofs": pb.n_dofs, "n_cells": pb.n_cells, "forward_s": round(t1 - t0, 4),
+            "backward_s": round(t2 - t1, 4), "fd_directions": fd_directions, "fd_rel_err": err}
+
+
+def vmult_rate(cells, degree, variant, prec, reps=10, seed=77):
+    """Device-timed vmult rate of one caching variant on a cells^3 unit cube
+    (mu in {1, 10} per cell, smooth displacement bounded by 0.01, bottom
+    clamped): GDoF/s and the fraction of the measured HBM bandwidth for the
+    variant's algorithmic bytes."""
+    import torch
+    import lsmf
+    mesh = lsmf.Mesh("box", (cells,) * 3, 0, degree=degree)
+    mesh.set_dirichlet([(4, 7)])
+    n_cells, n_nodes, n_dofs = mesh.info()
+    X, _, _ = mesh.arrays()
+    dt = torch.float64 if prec == "fp64" else torch.float32
+    u = torch.tensor(smooth_field(X, seed).reshape(-1), device="cuda", dtype=dt)
+    op = lsmf.NeoHookOperator(mesh, variant, 1, prec)
+    op.set_material(np.random.default_rng(seed).choice([1.0, 10.0], size=n_cells), NU)
+    op.cache(u)
+    src = torch.tensor(np.random.default_rng(seed + 1).uniform(-1, 1, n_dofs), device="cuda", dtype=dt)
+    dst = torch.empty_like(src)
+    stream = torch.cuda.current_stream()
+    op.set_stream(stream)
+    for _ in range(3):
+        op.vmult(dst, src)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        op.vmult(dst, src)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    by = alg_bytes(variant, 8 if prec == "fp64" else 4, n_nodes, n_cells * (degree + 1) ** 3, n_cells)
+    peak, _ = measured_peak()
+    del op
+    return {"n_dofs": n_dofs, "ms": round(ms, 4), "gdofs": round(n_dofs / (ms * 1e-3) / 1e9, 3),
+            "frac_hbm": round(by / (ms * 1e-3) / 1e9 / peak, 3)}
+
+
+def inclusions_prm(level_precision, cells=16, refinements=3):
+    """128^3 Q2 unit cube (50,923,779 DoFs): bottom clamped, top displaced
+    by -0.01 in z (first of 10 load steps), FP64 outer CG to 1e-8, Chebyshev
+    degree 4 smoother on FP32 or FP64 levels; mu is set per cell afterwards."""
+    return voids_prm(level_precision, cells, refinements).replace(
+        "  set Void spheres = 16, 0.08, 2024\n", "")
+
+
+def inclusion_mu(coarse=16, refinements=3, seed=99, n_spheres=32, target_fraction=0.2):
+    """mu = 10 in seeded spheres (about 20 % of the volume), 1 elsewhere, per
+    fine cell of the structured unit cube (cell centres), in the cell order
+    of the problem's mesh (the same coarse cells and refinements)."""
+    import lsmf
+    rng = np.random.default_rng(seed)
+    r = (target_fraction * 3.0 / (4.0 * np.pi * n_spheres)) ** (1.0 / 3.0)
+    centres = rng.uniform(0, 1, (n_spheres, 3))
+    mesh = lsmf.Mesh("box", (coarse,) * 3, refinements, degree=1)
+    _, _, ijk = mesh.arrays()
+    xc = (ijk + 0.5) / (coarse << refinements)
+    inside = np.zeros(len(xc), dtype=bool)
+    for c in centres:
+        inside |= np.sum((xc - c) ** 2, axis=1) <= r * r
+    return np.where(inside, 10.0, 1.0), float(inside.mean())
+
+
+def c5_measurements(repeats=3):
+    """The large configurations: vmult rates at 128^3 Q2 and 48^3 Q4
+    (tensor4, FP64 and FP32), and one Newton iteration of the 128^3 Q2
+    inclusion problem with FP32 and with FP64 GMG levels."""
+    import lsmf
+    out = {"vmult": {}}
+    for cells, degree in ((128, 2), (48, 4)):
+        for prec in ("fp64", "fp32"):
+            out["vmult"]["%d^3_Q%d_tensor4_%s" % (cells, degree, prec)] = vmult_rate(cells, degree, "tensor4", prec)
+    mu, frac = inclusion_mu()
+    sols = {}
+    for form, prec in (("fp32_gmg", "float"), ("fp64_gmg", "double")):
+        pb = lsmf.Problem(inclusions_prm(prec))
+        pb.set_mu(mu)
+        runs = []
+        for _ in range(repeats):
+            res = pb.run()
+            st = res["steps"][0]
+            total = res["time_residual"] + res["time_setup"] + res["time_solve"]
+            runs.append((total / max(1, st["newton_iterations"]), res, st))
+        runs.sort(key=lambda r: r[0])
+        per_step, res, st = runs[len(runs) // 2]
+        out[form] = {"n_dofs": pb.n_dofs, "newton_iterations": st["newton_iterations"],
+                     "cg_iterations": st["cg_iterations"], "s_per_newton_step": round(per_step, 4),
+                     "setup_s": round(res["time_setup"], 4), "solve_s": round(res["time_solve"], 4)}
+        sols[form] = pb.solution()
+        del pb
+    a, b = sols["fp32_gmg"], sols["fp64_gmg"]
+    out["speedup_fp32_over_fp64"] = round(out["fp64_gmg"]["s_per_newton_step"] / out["fp32_gmg"]["s_per_newton_step"], 3)
+    out["solution_rel_diff"] = float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+    out["workload"] = ("inclusions: 128^3 Q2 unit cube, mu = 10 in 32 seeded spheres (%.1f %% of the cells), "
+                       "tensor4, first load step, CG to 1e-8" % (100 * frac))
+    return out
+
+
 # ---------------------------------------------------------------- GPU (lsmf)
 def run_lsmf(args):
     import torch
@@ -422,6 +578,10 @@ def run_lsmf(args):
         torch.cuda.synchronize()
         newton = newton_step_times()
 
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_times()
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -440,7 +600,7 @@ def run_lsmf(args):
                            "l2": "inputs larger than L2 (2.9 GB cache tables), no flush"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": 2 * args.steps, "clocks": clocks, "variants": variants,
-                "newton_step": newton}
+                "newton_step": newton, "adjoint": adjoint}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -461,9 +621,15 @@ def main():
     ap.add_argument("--newton-cells", type=int, default=15, help="coarse cells per direction of the voids mesh")
     ap.add_argument("--newton-refinements", type=int, default=2)
     ap.add_argument("--cells", type=int, default=N_CELLS_1D, help="cells per direction (64 = the benchmark)")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-gradient timing")
+    ap.add_argument("--c5", action="store_true",
+                    help="only the large configurations (128^3 Q2, 48^3 Q4 vmults; 128^3 inclusion Newton step)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.c5:
+        print(json.dumps(c5_measurements()), flush=True)
+        return 0
     if args.newton_only:
         print(json.dumps(newton_step_times(args.newton_cells, args.newton_refinements)), flush=True)
         return 0

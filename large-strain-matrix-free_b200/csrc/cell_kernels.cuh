@@ -95,9 +95,10 @@ struct SFR {
   static constexpr int SZP = 9 * NQ;
   static constexpr int SZ = SZP + 2 * NA + 3 * NB;
 
-  // v[r][i]: value of component c at node (i, j, k) for x row r = lane + 32 r
-  static __device__ __forceinline__ void eval(const TabT<P, Q, T> &t, const T v[RPL][N1], T *slab, int lane,
-                                              T G[QPL][3][3]) {
+  // v[r][i]: value of component c at node (i, j, k) for x row r = lane + 32 r;
+  // the reference gradients are left in the point block of the slab,
+  // Pt[(c * 3 + e) * NQ + q]
+  static __device__ __forceinline__ void eval_pt(const TabT<P, Q, T> &t, const T v[RPL][N1], T *slab, int lane) {
     T *Pt = slab, *A = slab + SZP, *B = A + 2 * NA;
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
@@ -167,6 +168,13 @@ struct SFR {
       }
     }
     __syncwarp();
+  }
+
+  // eval_pt, then the gradients of the points lane + 32 l into registers
+  static __device__ __forceinline__ void eval(const TabT<P, Q, T> &t, const T v[RPL][N1], T *slab, int lane,
+                                              T G[QPL][3][3]) {
+    eval_pt(t, v, slab, lane);
+    const T *Pt = slab;
 #pragma unroll
     for (int l = 0; l < QPL; ++l) {
       const int q = lane + 32 * l;
@@ -183,7 +191,7 @@ struct SFR {
   // per-point H -> out[r][i] for x row r (component c, node (i, j, k))
   static __device__ __forceinline__ void integrate(const TabT<P, Q, T> &t, const T H[QPL][3][3], T *slab, int lane,
                                                    T out[RPL][N1]) {
-    T *Pt = slab, *Y = slab + SZP, *Z = Y + 2 * NA;
+    T *Pt = slab;
 #pragma unroll
     for (int l = 0; l < QPL; ++l) {
       const int q = lane + 32 * l;
@@ -194,6 +202,12 @@ struct SFR {
           for (int e = 0; e < 3; ++e) Pt[(c * 3 + e) * NQ + q] = H[l][c][e];
       }
     }
+    integrate_pt(t, slab, lane, out);
+  }
+
+  // the same with H already in the point block of the slab
+  static __device__ __forceinline__ void integrate_pt(const TabT<P, Q, T> &t, T *slab, int lane, T out[RPL][N1]) {
+    T *Pt = slab, *Y = slab + SZP, *Z = Y + 2 * NA;
     __syncwarp();
     for (int row = lane; row < ZR; row += 32) {
       const int qyx = row % (Q * Q), c = row / (Q * Q);

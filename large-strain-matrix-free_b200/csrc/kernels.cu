@@ -370,6 +370,12 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
   using S = SFR<P, Q, T>;
   constexpr int N1 = P + 1, NN = S::NN, NQ = S::NQ, QPL = S::QPL, RPL = S::RPL, XR = S::XR;
   constexpr bool SCALAR = (VAR == VAR_SCALAR_F0 || VAR == VAR_SCALAR_F1);
+  // several points per lane (Q^3 > 32): the gradients stay in the slab's
+  // point block and each point is read, transformed and overwritten there
+  // in turn, instead of holding 2 x 9 x QPL values in registers (the FP64 Q4
+  // kernel otherwise runs out of registers); the scalar variants also need
+  // the displacement gradients and keep the register form
+  constexpr bool PT_SMEM = !SCALAR && QPL >= 2;
   const int WPB = blockDim.x >> 5;
   extern __shared__ __align__(128) unsigned char smem[];
   const int rec_elems = a.ncomp * NQ;
@@ -452,7 +458,8 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
     if (cell + nw < a.n_cells) prefetch(cell + nw);
     T G[QPL][3][3], GU[QPL][3][3];
     if (SCALAR) S::eval(tab, vu, slab, lane, GU);
-    S::eval(tab, v, slab, lane, G);
+    if (PT_SMEM) S::eval_pt(tab, v, slab, lane);
+    else S::eval(tab, v, slab, lane, G);
     const T *rec;
     if (STAGES > 0) {
       if (!mbar_wait_bounded(&bar[s], parity)) {
@@ -469,7 +476,7 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
     T mu = 0, lambda = 0, kappa = 0;
     if (SCALAR || VAR == VAR_SCALAR_REF) material<T>(a.mu[cell], a.nu, mu, lambda, kappa);
     T H[QPL][3][3];
-#pragma unroll
+#pragma unroll(PT_SMEM ? 1 : QPL)
     for (int l = 0; l < QPL; ++l) {
       const int q = lane + 32 * l;
 #pragma unroll
@@ -482,11 +489,16 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
 #pragma unroll
       for (int i = 0; i < 9; ++i) Ji[i / 3][i % 3] = r[(C_JINV + i) * NQ];
       const T jxw = r[C_JXW * NQ];
+      T Gq[3][3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int e = 0; e < 3; ++e) Gq[c][e] = PT_SMEM ? slab[(c * 3 + e) * NQ + q] : G[l][c][e];
       T g[3][3];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
-        for (int d = 0; d < 3; ++d) g[c][d] = G[l][c][0] * Ji[0][d] + G[l][c][1] * Ji[1][d] + G[l][c][2] * Ji[2][d];
+        for (int d = 0; d < 3; ++d) g[c][d] = Gq[c][0] * Ji[0][d] + Gq[c][1] * Ji[1][d] + Gq[c][2] * Ji[2][d];
       ScalarState<T> st;
       if (SCALAR) {
         T Jr[3][3];
@@ -508,7 +520,12 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
-        for (int e = 0; e < 3; ++e) H[l][c][e] = (Qm[c][0] * Ji[e][0] + Qm[c][1] * Ji[e][1] + Qm[c][2] * Ji[e][2]) * jxw;
+        for (int e = 0; e < 3; ++e) {
+          const T h = (Qm[c][0] * Ji[e][0] + Qm[c][1] * Ji[e][1] + Qm[c][2] * Ji[e][2]) * jxw;
+          // each lane overwrites only its own points
+          if (PT_SMEM) slab[(c * 3 + e) * NQ + q] = h;
+          else H[l][c][e] = h;
+        }
     }
     if (STAGES > 0) {
       __syncwarp();  // every lane is done reading stage[s]
@@ -522,7 +539,8 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
       }
     }
     T out[RPL][N1];
-    S::integrate(tab, H, slab, lane, out);
+    if (PT_SMEM) S::integrate_pt(tab, slab, lane, out);
+    else S::integrate(tab, H, slab, lane, out);
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
       const int row = lane + 32 * r;
