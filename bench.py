@@ -253,16 +253,16 @@ def adjoint_prm(cells=8, refinements=2):
     """Adjoint workload: unit cube, cells^3 coarse cells refined twice (32^3
     Q2 cells, 823,875 DoFs), bottom clamped, traction (0.02 t, 0, -0.05 t) on
     the top face, one load step solved to a tight Newton tolerance (relative
-    1e-14, no absolute stop) with FP32 GMG levels and an FP64 outer CG to
-    1e-12."""
+    residual 1e-12 and update 1e-10, no absolute stop) with FP32 GMG levels
+    and an FP64 outer CG to 1e-12."""
     keys = [("Finite element system", [("Polynomial degree", 2), ("Quadrature order", 3)]),
             ("Geometry", [("Dimension", 3), ("Type", "Box"), ("Box cells", "%d, %d, %d" % ((cells,) * 3)),
                           ("Global refinement", refinements)]),
             ("Material properties", [("Shear modulus", 1.0), ("Poisson's ratio", 0.3), ("Formulation", 1)]),
             ("Linear solver", [("Solver type", "MF_CG"), ("Residual", 1e-12), ("Preconditioner type", "gmg"),
                                ("MF caching", "tensor4"), ("MF level precision", "float")]),
-            ("Nonlinear solver", [("Max iterations Newton-Raphson", 25), ("Tolerance force", 1e-14),
-                                  ("Tolerance displacement", 1e-14), ("Absolute tolerance force", 1e-17),
+            ("Nonlinear solver", [("Max iterations Newton-Raphson", 25), ("Tolerance force", 1e-12),
+                                  ("Tolerance displacement", 1e-10), ("Absolute tolerance force", 1e-17),
                                   ("Absolute tolerance displacement", 1e-17)]),
             ("Boundary conditions", [("Dirichlet IDs and expressions", "4:0,0,0"),
                                      ("Dirichlet IDs and component mask", "4:true,true,true"),

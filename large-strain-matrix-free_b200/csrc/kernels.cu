@@ -807,10 +807,15 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask) {
   const size_t rec_bytes = (size_t)op->ncomp * S::NQ * sizeof(T);
   const TabT<P, Q, T> tabt = make_tabt<P, Q, T>(op->mesh->basis);
   auto wbytes = [&](int st) { return ((st * rec_bytes + 8 * (st > 0 ? st : 1) + SR::SZ * sizeof(T) + 127) / 128) * 128; };
-  // defaults measured on B200 at 64^3 Q2 (ring depth, warps per block):
-  // tensor4 streams 52 values per point and wants the bulk-copy ring;
-  // tensor2 and scalar are latency / FP64 bound and run best on plain loads
-  int stages = op->stages >= 0 ? op->stages : ((VAR == VAR_TENSOR4 || VAR == VAR_TENSOR4_NS) ? 1 : 0);
+  // defaults measured on B200 (ring depth x warps per block swept for
+  // Q2 / Q3 / Q4 at 64^3 / 48^3 / 48^3 cells): the variants that stream a
+  // large record per point (tensor4, tensor4_ns) and scalar_referential
+  // (whose collocation gradient reads the record out of order) want the
+  // one-stage bulk-copy ring while a record fits in 24 KB; larger records
+  // (Q3 FP64, Q4) cost more occupancy than the ring gains and run on plain
+  // loads, as do tensor2 and scalar (latency / FP64 bound)
+  const bool ring_variant = VAR == VAR_TENSOR4 || VAR == VAR_TENSOR4_NS || VAR == VAR_SCALAR_REF;
+  int stages = op->stages >= 0 ? op->stages : ((ring_variant && rec_bytes <= 24 * 1024) ? 1 : 0);
   const int max_warps = op->max_warps > 0 ? op->max_warps : (VAR == VAR_TENSOR2 ? 8 : 4);
   if (rec_bytes % 16 != 0) stages = 0;
   // fewer stages when the ring would leave fewer than 4 warps per block

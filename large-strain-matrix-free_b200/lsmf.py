@@ -261,8 +261,10 @@ class NeoHookOperator:
         check(lib().lsmf_operator_precondition_jacobi(self.h, _dptr(dst), _dptr(src), omega))
 
     def set_pipeline(self, stages):
-        """Ring depth of the bulk-copy (TMA) record pipeline in vmult (default
-        2; 0 = plain loads).  True/False select 2/0."""
+        """Ring depth (0..3) of the bulk-copy record pipeline in vmult; 0 =
+        plain loads, -1 = the measured default (one stage for the large-record
+        variants while a record fits in 24 KB, else plain loads).  True/False
+        select 2/0."""
         if stages is True:
             stages = 2
         check(lib().lsmf_operator_set_option(self.h, 1, int(stages)))
