@@ -75,6 +75,39 @@ __device__ __forceinline__ void collocation_F(const T *__restrict__ rec, int q, 
       F[c][d] = G[c][0] * Ji[0][d] + G[c][1] * Ji[1][d] + G[c][2] * Ji[2][d] + (c == d ? T(1) : T(0));
 }
 
+// Shared-memory layout of the row sweeps, chosen per (degree, element size)
+// by a wavefront count of every warp access of the sweeps (32 banks of 4
+// bytes; 8-byte words served per half warp) so that the transposes between
+// sweeps are free of bank conflicts where the unpadded tensors allow it:
+//   Y0..Y2: order in which the y sweep enumerates its rows (c, k, qx) over
+//           the lanes, fastest first (ids 0 = c, 1 = k, 2 = qx);
+//   Z0..Z2: the same for the z sweep rows (0 = c, 1 = qy, 2 = qx);
+//   NQP:    stride of the 9 per-point blocks (c, e) of the point tensor.
+template <int P, int ES>
+struct SFRLayout {  // generic: the natural orders, no padding
+  static constexpr int Y0 = 2, Y1 = 1, Y2 = 0, Z0 = 2, Z1 = 1, Z2 = 0;
+  static constexpr int NQP = (P + 1) * (P + 1) * (P + 1);
+};
+// Q1 / Q2 with 8-byte (FP64) and 4-byte (FP32) entries.  Wavefronts per
+// cell of the sweeps and point accesses, natural -> chosen: Q2 FP64 306 ->
+// 192 (conflict-free), Q2 FP32 162 -> 144, Q1 FP64 122 -> 110.  For Q3 / Q4
+// the best orders with unpadded A / B save under 10 % of the wavefronts and
+// measured slower (FP32 Q4 0.73 -> 1.08 ms), so they keep the natural layout.
+template <> struct SFRLayout<1, 8> { static constexpr int Y0 = 0, Y1 = 1, Y2 = 2, Z0 = 0, Z1 = 1, Z2 = 2, NQP = 9; };
+template <> struct SFRLayout<1, 4> { static constexpr int Y0 = 0, Y1 = 1, Y2 = 2, Z0 = 0, Z1 = 1, Z2 = 2, NQP = 8; };
+template <> struct SFRLayout<2, 8> { static constexpr int Y0 = 1, Y1 = 0, Y2 = 2, Z0 = 0, Z1 = 2, Z2 = 1, NQP = 41; };
+template <> struct SFRLayout<2, 4> { static constexpr int Y0 = 0, Y1 = 1, Y2 = 2, Z0 = 0, Z1 = 1, Z2 = 2, NQP = 29; };
+
+// row -> its three indices (by id) for an enumeration (I0 fastest, I2
+// slowest) over index ranges D[id]
+template <int I0, int I1, int I2, int DA, int DB, int DC>
+__device__ __forceinline__ void decode_row(int row, int idx[3]) {
+  constexpr int D[3] = {DA, DB, DC};
+  idx[I0] = row % D[I0];
+  idx[I1] = (row / D[I0]) % D[I1];
+  idx[I2] = row / (D[I0] * D[I1]);
+}
+
 // Sum factorisation with one 1D line per lane ("row" sweeps).  Each sweep
 // maps lane -> row of the tensor it produces and unrolls the 1D contraction
 // completely; shared memory only carries the transposes between sweeps.
@@ -84,7 +117,9 @@ __device__ __forceinline__ void collocation_F(const T *__restrict__ rec, int q, 
 // Slab layout (elements of T): [9*NQ points][2*NA][3*NB].
 template <int P, int Q, typename T>
 struct SFR {
+  using LY = SFRLayout<P, (int)sizeof(T)>;
   static constexpr int N1 = P + 1, NN = N1 * N1 * N1, NQ = Q * Q * Q;
+  static constexpr int NQP = (Q == P + 1) ? LY::NQP : NQ;  // point-block stride
   static constexpr int QPL = (NQ + 31) / 32;
   static constexpr int XR = 3 * N1 * N1;      // x rows (c,k,j)
   static constexpr int YR = 3 * N1 * Q;       // y rows (c,k,qx)
@@ -92,12 +127,12 @@ struct SFR {
   static constexpr int RPL = (XR + 31) / 32;  // x rows per lane
   static constexpr int NA = 3 * N1 * N1 * Q;
   static constexpr int NB = 3 * N1 * Q * Q;
-  static constexpr int SZP = 9 * NQ;
+  static constexpr int SZP = 9 * NQP;
   static constexpr int SZ = SZP + 2 * NA + 3 * NB;
 
   // v[r][i]: value of component c at node (i, j, k) for x row r = lane + 32 r;
   // the reference gradients are left in the point block of the slab,
-  // Pt[(c * 3 + e) * NQ + q]
+  // Pt[(c * 3 + e) * NQP + q]
   static __device__ __forceinline__ void eval_pt(const TabT<P, Q, T> &t, const T v[RPL][N1], T *slab, int lane) {
     T *Pt = slab, *A = slab + SZP, *B = A + 2 * NA;
 #pragma unroll
@@ -119,7 +154,9 @@ struct SFR {
     }
     __syncwarp();
     for (int row = lane; row < YR; row += 32) {
-      const int qx = row % Q, ck = row / Q;  // ck = c*N1 + k
+      int ix[3];
+      decode_row<LY::Y0, LY::Y1, LY::Y2, 3, N1, Q>(row, ix);
+      const int qx = ix[2], ck = ix[0] * N1 + ix[1];  // ck = c*N1 + k
       T a0[N1], a1[N1];
 #pragma unroll
       for (int j = 0; j < N1; ++j) {
@@ -143,7 +180,9 @@ struct SFR {
     }
     __syncwarp();
     for (int row = lane; row < ZR; row += 32) {
-      const int qyx = row % (Q * Q), c = row / (Q * Q);
+      int ix[3];
+      decode_row<LY::Z0, LY::Z1, LY::Z2, 3, Q, Q>(row, ix);
+      const int qyx = ix[1] * Q + ix[2], c = ix[0];
       T b00[N1], b01[N1], b10[N1];
 #pragma unroll
       for (int k = 0; k < N1; ++k) {
@@ -162,9 +201,9 @@ struct SFR {
           gz += t.D[qz][k] * b00[k];
         }
         const int q = qz * Q * Q + qyx;
-        Pt[(c * 3 + 0) * NQ + q] = gx;
-        Pt[(c * 3 + 1) * NQ + q] = gy;
-        Pt[(c * 3 + 2) * NQ + q] = gz;
+        Pt[(c * 3 + 0) * NQP + q] = gx;
+        Pt[(c * 3 + 1) * NQP + q] = gy;
+        Pt[(c * 3 + 2) * NQP + q] = gz;
       }
     }
     __syncwarp();
@@ -182,7 +221,7 @@ struct SFR {
 #pragma unroll
         for (int c = 0; c < 3; ++c)
 #pragma unroll
-          for (int e = 0; e < 3; ++e) G[l][c][e] = Pt[(c * 3 + e) * NQ + q];
+          for (int e = 0; e < 3; ++e) G[l][c][e] = Pt[(c * 3 + e) * NQP + q];
       }
     }
     __syncwarp();
@@ -199,7 +238,7 @@ struct SFR {
 #pragma unroll
         for (int c = 0; c < 3; ++c)
 #pragma unroll
-          for (int e = 0; e < 3; ++e) Pt[(c * 3 + e) * NQ + q] = H[l][c][e];
+          for (int e = 0; e < 3; ++e) Pt[(c * 3 + e) * NQP + q] = H[l][c][e];
       }
     }
     integrate_pt(t, slab, lane, out);
@@ -210,14 +249,16 @@ struct SFR {
     T *Pt = slab, *Y = slab + SZP, *Z = Y + 2 * NA;
     __syncwarp();
     for (int row = lane; row < ZR; row += 32) {
-      const int qyx = row % (Q * Q), c = row / (Q * Q);
+      int ix[3];
+      decode_row<LY::Z0, LY::Z1, LY::Z2, 3, Q, Q>(row, ix);
+      const int qyx = ix[1] * Q + ix[2], c = ix[0];
       T hx[Q], hy[Q], hz[Q];
 #pragma unroll
       for (int qz = 0; qz < Q; ++qz) {
         const int q = qz * Q * Q + qyx;
-        hx[qz] = Pt[(c * 3 + 0) * NQ + q];
-        hy[qz] = Pt[(c * 3 + 1) * NQ + q];
-        hz[qz] = Pt[(c * 3 + 2) * NQ + q];
+        hx[qz] = Pt[(c * 3 + 0) * NQP + q];
+        hy[qz] = Pt[(c * 3 + 1) * NQP + q];
+        hz[qz] = Pt[(c * 3 + 2) * NQP + q];
       }
 #pragma unroll
       for (int k = 0; k < N1; ++k) {
@@ -236,7 +277,9 @@ struct SFR {
     }
     __syncwarp();
     for (int row = lane; row < YR; row += 32) {
-      const int qx = row % Q, ck = row / Q;
+      int ix[3];
+      decode_row<LY::Y0, LY::Y1, LY::Y2, 3, N1, Q>(row, ix);
+      const int qx = ix[2], ck = ix[0] * N1 + ix[1];
       T zx[Q], zy[Q], zz[Q];
 #pragma unroll
       for (int qy = 0; qy < Q; ++qy) {

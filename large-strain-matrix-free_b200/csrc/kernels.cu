@@ -493,7 +493,7 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
-        for (int e = 0; e < 3; ++e) Gq[c][e] = PT_SMEM ? slab[(c * 3 + e) * NQ + q] : G[l][c][e];
+        for (int e = 0; e < 3; ++e) Gq[c][e] = PT_SMEM ? slab[(c * 3 + e) * S::NQP + q] : G[l][c][e];
       T g[3][3];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
@@ -523,7 +523,7 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
         for (int e = 0; e < 3; ++e) {
           const T h = (Qm[c][0] * Ji[e][0] + Qm[c][1] * Ji[e][1] + Qm[c][2] * Ji[e][2]) * jxw;
           // each lane overwrites only its own points
-          if (PT_SMEM) slab[(c * 3 + e) * NQ + q] = h;
+          if (PT_SMEM) slab[(c * 3 + e) * S::NQP + q] = h;
           else H[l][c][e] = h;
         }
     }
