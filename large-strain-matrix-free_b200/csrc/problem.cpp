@@ -255,6 +255,12 @@ struct Timer {
   }
 };
 
+// "gmg-gc" (global coarsening, mf_elasticity.h:1597-1632, 1892-1916) builds
+// its levels by coarsening the triangulation; on the structured meshes here,
+// which are refined globally and have no hanging nodes, that sequence is the
+// multigrid level hierarchy itself, the two-level transfers are the nested
+// Q_p interpolation with the levels' homogeneous Dirichlet constraints, and
+// the preconditioner is the same as "gmg"
 int precond_code(const std::string &s) { return s == "none" ? 0 : (s == "jacobi" ? 1 : 2); }
 
 }  // namespace
@@ -388,8 +394,8 @@ extern "C" {
 static lsmf_status validate_params(const ProblemParams &P, int &caching) {
   if (P.dim != 3) { set_error("only Dimension = 3 is supported"); return LSMF_ERR_UNSUPPORTED; }
   if (P.solver_type != "MF_CG") { set_error("Solver type " + P.solver_type + " is not supported (MF_CG only)"); return LSMF_ERR_UNSUPPORTED; }
-  if (P.precond != "jacobi" && P.precond != "gmg" && P.precond != "none") {
-    set_error("Preconditioner type " + P.precond + " is not supported (jacobi | gmg | none)");
+  if (P.precond != "jacobi" && P.precond != "gmg" && P.precond != "gmg-gc" && P.precond != "none") {
+    set_error("Preconditioner type " + P.precond + " is not supported (jacobi | gmg | gmg-gc | none)");
     return LSMF_ERR_UNSUPPORTED;
   }
   if (P.caching == "scalar") caching = LSMF_CACHE_SCALAR;
@@ -473,7 +479,7 @@ lsmf_status lsmf_problem_create(const char *text, lsmf_problem **out) {
     delete pb;
     return s;
   }
-  if (P.precond == "gmg") {
+  if (precond_code(P.precond) == 2) {
     lsmf_gmg_desc gd{};
     gd.caching = caching;
     gd.formulation = P.formulation;

@@ -46,6 +46,12 @@ def test_prm_valid():
     assert st == 0, msg
 
 
+@pytest.mark.parametrize("precond", ["gmg", "gmg-gc", "jacobi", "none"])
+def test_prm_every_preconditioner(precond):
+    st, msg = lsmf.prm_validate(prm_text(dict(BASE, **{"Preconditioner type": precond})))
+    assert st == 0, msg
+
+
 @pytest.mark.parametrize("caching", ["scalar", "tensor2", "tensor4", "scalar_referential", "tensor4_ns"])
 def test_prm_every_caching(caching):
     st, msg = lsmf.prm_validate(prm_text(dict(BASE, **{"MF caching": caching})))

@@ -70,6 +70,17 @@ def test_newton_gmg_matches_oracle(precision):
     assert np.max(np.abs(u - ref["u"])) <= 1e-7 * np.max(np.abs(ref["u"]))
 
 
+def test_newton_gmg_gc_equals_gmg():
+    # global coarsening on a globally refined mesh builds the same levels and
+    # transfers, so the solve is the same
+    pb = lsmf.Problem(_cook_prm("float", precond="gmg-gc", end=0.2, dt=0.2))
+    res = pb.run()
+    pb2 = lsmf.Problem(_cook_prm("float", precond="gmg", end=0.2, dt=0.2))
+    res2 = pb2.run()
+    assert [s["newton_iterations"] for s in res["steps"]] == [s["newton_iterations"] for s in res2["steps"]]
+    assert np.max(np.abs(pb.solution() - pb2.solution())) <= 1e-7 * np.max(np.abs(pb2.solution()))
+
+
 @pytest.mark.parametrize("caching", ["tensor2", "scalar", "scalar_referential", "tensor4_ns"])
 def test_newton_other_cachings(caching):
     pb = lsmf.Problem(_cook_prm("float", caching=caching, end=0.2, dt=0.2))
