@@ -405,6 +405,24 @@ def c5_measurements(repeats=3):
     return out
 
 
+def max_over_ranks(t_ms, dist, device):
+    """The slowest rank's time (every rank takes part; a single process
+    returns its own)."""
+    if not dist:
+        return t_ms
+    import torch
+    tt = torch.tensor([float(t_ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def job_rate(world, n_dofs, steps, t_ms):
+    """Whole-job GDoF/s: every rank (replica) applies the operator to its own
+    n_dofs vector once per step; t_ms is the max-over-ranks time of `steps`
+    steps."""
+    return world * n_dofs * steps / (t_ms * 1e-3) / 1e9
+
+
 # ---------------------------------------------------------------- GPU (lsmf)
 def run_lsmf(args):
     import torch
@@ -475,11 +493,8 @@ def run_lsmf(args):
     torch.cuda.synchronize()
     apply_ms = float(np.mean([a.elapsed_time(b) for a, b in ts]))
     clocks = sampler.stop()
-    if dist:
-        tt = torch.tensor([t_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
-    value = world * n_dofs * args.steps / (t_ms * 1e-3) / 1e9
+    t_ms = max_over_ranks(t_ms, dist, "cuda")
+    value = job_rate(world, n_dofs, args.steps, t_ms)
 
     # per-variant rates (same mesh / inputs)
     variants = {}
@@ -556,11 +571,8 @@ def run_lsmf(args):
     torch.cuda.synchronize()
     e2e_ms = a.elapsed_time(b) / args.steps
     assert torch.allclose(d_dst[(args.steps - 1) % nbuf], dst_pin[(args.steps - 1) % nbuf].cuda())
-    if dist:
-        tt = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
-    e2e = {"value": world * n_dofs / (e2e_ms * 1e-3) / 1e9, "unit": "GDoF/s",
+    e2e_ms = max_over_ranks(e2e_ms, dist, "cuda")
+    e2e = {"value": job_rate(world, n_dofs, 1, e2e_ms), "unit": "GDoF/s",
            "h2d_bytes_per_step": n_dofs * 8, "d2h_bytes_per_step": n_dofs * 8,
            "pipelining": "H2D(i+1) and D2H(i-1) overlap vmult(i), double-buffered"}
     lib.lsmf_operator_set_stream(op.h, lsmf.vp(stream.cuda_stream))
