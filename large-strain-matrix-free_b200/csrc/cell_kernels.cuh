@@ -79,24 +79,44 @@ __device__ __forceinline__ void collocation_F(const T *__restrict__ rec, int q, 
 // by a wavefront count of every warp access of the sweeps (32 banks of 4
 // bytes; 8-byte words served per half warp) so that the transposes between
 // sweeps are free of bank conflicts where the unpadded tensors allow it:
-//   Y0..Y2: order in which the y sweep enumerates its rows (c, k, qx) over
-//           the lanes, fastest first (ids 0 = c, 1 = k, 2 = qx);
+//   X0..X2: order in which the x sweep (and the gather / scatter) enumerates
+//           its rows (c, k, j) over the lanes, fastest first (ids 0 = c,
+//           1 = k, 2 = j);
+//   Y0..Y2: the same for the y sweep rows (0 = c, 1 = k, 2 = qx);
 //   Z0..Z2: the same for the z sweep rows (0 = c, 1 = qy, 2 = qx);
+//   AC, AK, AJ, AQ: strides of the x-sweep output A[c][k][j][qx] (and of
+//           the y-sweep output of integrate);
+//   BC, BK, BY, BX: strides of the y-sweep output B[c][k][qy][qx] (and of
+//           the z-sweep output of integrate);
 //   NQP:    stride of the 9 per-point blocks (c, e) of the point tensor.
 template <int P, int ES>
 struct SFRLayout {  // generic: the natural orders, no padding
-  static constexpr int Y0 = 2, Y1 = 1, Y2 = 0, Z0 = 2, Z1 = 1, Z2 = 0;
-  static constexpr int NQP = (P + 1) * (P + 1) * (P + 1);
+  static constexpr int N1 = P + 1;
+  static constexpr int X0 = 2, X1 = 1, X2 = 0, Y0 = 2, Y1 = 1, Y2 = 0, Z0 = 2, Z1 = 1, Z2 = 0;
+  static constexpr int AC = N1 * N1 * N1, AK = N1 * N1, AJ = N1, AQ = 1;
+  static constexpr int BC = N1 * N1 * N1, BK = N1 * N1, BY = N1, BX = 1;
+  static constexpr int NQP = N1 * N1 * N1;
 };
 // Q1 / Q2 with 8-byte (FP64) and 4-byte (FP32) entries.  Wavefronts per
 // cell of the sweeps and point accesses, natural -> chosen: Q2 FP64 306 ->
-// 192 (conflict-free), Q2 FP32 162 -> 144, Q1 FP64 122 -> 110.  For Q3 / Q4
-// the best orders with unpadded A / B save under 10 % of the wavefronts and
-// measured slower (FP32 Q4 0.73 -> 1.08 ms), so they keep the natural layout.
-template <> struct SFRLayout<1, 8> { static constexpr int Y0 = 0, Y1 = 1, Y2 = 2, Z0 = 0, Z1 = 1, Z2 = 2, NQP = 9; };
-template <> struct SFRLayout<1, 4> { static constexpr int Y0 = 0, Y1 = 1, Y2 = 2, Z0 = 0, Z1 = 1, Z2 = 2, NQP = 8; };
-template <> struct SFRLayout<2, 8> { static constexpr int Y0 = 1, Y1 = 0, Y2 = 2, Z0 = 0, Z1 = 2, Z2 = 1, NQP = 41; };
-template <> struct SFRLayout<2, 4> { static constexpr int Y0 = 0, Y1 = 1, Y2 = 2, Z0 = 0, Z1 = 1, Z2 = 2, NQP = 29; };
+// 192 and Q2 FP32 162 -> 96 (both conflict-free), Q1 FP64 122 -> 110.  For
+// Q3 / Q4 the best orders with unpadded A / B save under 10 % of the
+// wavefronts and measured slower (FP32 Q4 0.73 -> 1.08 ms), so they keep the
+// natural layout.
+template <int P, int Y0_, int Y1_, int Y2_, int Z0_, int Z1_, int Z2_, int NQP_>
+struct SFRLayoutYZ : SFRLayout<P, 0> {
+  static constexpr int Y0 = Y0_, Y1 = Y1_, Y2 = Y2_, Z0 = Z0_, Z1 = Z1_, Z2 = Z2_, NQP = NQP_;
+};
+template <> struct SFRLayout<1, 8> : SFRLayoutYZ<1, 0, 1, 2, 0, 1, 2, 9> {};
+template <> struct SFRLayout<1, 4> : SFRLayoutYZ<1, 0, 1, 2, 0, 1, 2, 8> {};
+template <> struct SFRLayout<2, 8> : SFRLayoutYZ<2, 1, 0, 2, 0, 2, 1, 41> {};
+// FP32 Q2: x rows with the component fastest (the three components of a node
+// are gathered by neighbouring lanes), A[j][c][k][qx], B[k][c][qx][qy]
+template <> struct SFRLayout<2, 4> : SFRLayoutYZ<2, 0, 1, 2, 0, 1, 2, 29> {
+  static constexpr int X0 = 0, X1 = 1, X2 = 2;
+  static constexpr int AC = 9, AK = 3, AJ = 27, AQ = 1;
+  static constexpr int BC = 9, BK = 27, BY = 1, BX = 3;
+};
 
 // row -> its three indices (by id) for an enumeration (I0 fastest, I2
 // slowest) over index ranges D[id]
@@ -133,12 +153,27 @@ struct SFR {
   // v[r][i]: value of component c at node (i, j, k) for x row r = lane + 32 r;
   // the reference gradients are left in the point block of the slab,
   // Pt[(c * 3 + e) * NQP + q]
+  // x row (component c, node line (k, j)) of a lane: row -> (c, k, j)
+  static __device__ __forceinline__ void x_row(int row, int &c, int &k, int &j) {
+    int ix[3];
+    decode_row<LY::X0, LY::X1, LY::X2, 3, N1, N1>(row, ix);
+    c = ix[0]; k = ix[1]; j = ix[2];
+  }
+  static __device__ __forceinline__ int a_at(int c, int k, int j, int qx) {
+    return c * LY::AC + k * LY::AK + j * LY::AJ + qx * LY::AQ;
+  }
+  static __device__ __forceinline__ int b_at(int c, int k, int qy, int qx) {
+    return c * LY::BC + k * LY::BK + qy * LY::BY + qx * LY::BX;
+  }
+
   static __device__ __forceinline__ void eval_pt(const TabT<P, Q, T> &t, const T v[RPL][N1], T *slab, int lane) {
     T *Pt = slab, *A = slab + SZP, *B = A + 2 * NA;
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
       const int row = lane + 32 * r;
       if (row < XR) {
+        int c, k, j;
+        x_row(row, c, k, j);
 #pragma unroll
         for (int qx = 0; qx < Q; ++qx) {
           T s0 = 0, s1 = 0;
@@ -147,8 +182,8 @@ struct SFR {
             s0 += t.N[qx][i] * v[r][i];
             s1 += t.D[qx][i] * v[r][i];
           }
-          A[row * Q + qx] = s0;
-          A[NA + row * Q + qx] = s1;
+          A[a_at(c, k, j, qx)] = s0;
+          A[NA + a_at(c, k, j, qx)] = s1;
         }
       }
     }
@@ -156,12 +191,12 @@ struct SFR {
     for (int row = lane; row < YR; row += 32) {
       int ix[3];
       decode_row<LY::Y0, LY::Y1, LY::Y2, 3, N1, Q>(row, ix);
-      const int qx = ix[2], ck = ix[0] * N1 + ix[1];  // ck = c*N1 + k
+      const int c = ix[0], k = ix[1], qx = ix[2];
       T a0[N1], a1[N1];
 #pragma unroll
       for (int j = 0; j < N1; ++j) {
-        a0[j] = A[(ck * N1 + j) * Q + qx];
-        a1[j] = A[NA + (ck * N1 + j) * Q + qx];
+        a0[j] = A[a_at(c, k, j, qx)];
+        a1[j] = A[NA + a_at(c, k, j, qx)];
       }
 #pragma unroll
       for (int qy = 0; qy < Q; ++qy) {
@@ -172,7 +207,7 @@ struct SFR {
           s01 += t.D[qy][j] * a0[j];
           s10 += t.N[qy][j] * a1[j];
         }
-        const int b = (ck * Q + qy) * Q + qx;
+        const int b = b_at(c, k, qy, qx);
         B[b] = s00;
         B[NB + b] = s01;
         B[2 * NB + b] = s10;
@@ -186,7 +221,7 @@ struct SFR {
       T b00[N1], b01[N1], b10[N1];
 #pragma unroll
       for (int k = 0; k < N1; ++k) {
-        const int b = (c * N1 + k) * Q * Q + qyx;
+        const int b = b_at(c, k, ix[1], ix[2]);
         b00[k] = B[b];
         b01[k] = B[NB + b];
         b10[k] = B[2 * NB + b];
@@ -269,7 +304,7 @@ struct SFR {
           sy += t.N[qz][k] * hy[qz];
           sz += t.D[qz][k] * hz[qz];
         }
-        const int z = (c * N1 + k) * Q * Q + qyx;
+        const int z = b_at(c, k, ix[1], ix[2]);
         Z[z] = sx;
         Z[NB + z] = sy;
         Z[2 * NB + z] = sz;
@@ -279,11 +314,11 @@ struct SFR {
     for (int row = lane; row < YR; row += 32) {
       int ix[3];
       decode_row<LY::Y0, LY::Y1, LY::Y2, 3, N1, Q>(row, ix);
-      const int qx = ix[2], ck = ix[0] * N1 + ix[1];
+      const int c = ix[0], k = ix[1], qx = ix[2];
       T zx[Q], zy[Q], zz[Q];
 #pragma unroll
       for (int qy = 0; qy < Q; ++qy) {
-        const int z = (ck * Q + qy) * Q + qx;
+        const int z = b_at(c, k, qy, qx);
         zx[qy] = Z[z];
         zy[qy] = Z[NB + z];
         zz[qy] = Z[2 * NB + z];
@@ -296,7 +331,7 @@ struct SFR {
           sx += t.N[qy][j] * zx[qy];
           so += t.D[qy][j] * zy[qy] + t.N[qy][j] * zz[qy];
         }
-        const int y = (ck * N1 + j) * Q + qx;
+        const int y = a_at(c, k, j, qx);
         Y[y] = sx;
         Y[NA + y] = so;
       }
@@ -306,11 +341,13 @@ struct SFR {
     for (int r = 0; r < RPL; ++r) {
       const int row = lane + 32 * r;
       if (row < XR) {
+        int c, k, j;
+        x_row(row, c, k, j);
         T yx[Q], yo[Q];
 #pragma unroll
         for (int qx = 0; qx < Q; ++qx) {
-          yx[qx] = Y[row * Q + qx];
-          yo[qx] = Y[NA + row * Q + qx];
+          yx[qx] = Y[a_at(c, k, j, qx)];
+          yo[qx] = Y[NA + a_at(c, k, j, qx)];
         }
 #pragma unroll
         for (int i = 0; i < N1; ++i) {

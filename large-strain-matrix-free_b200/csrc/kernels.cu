@@ -419,7 +419,9 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
     for (int r = 0; r < RPL; ++r) {
       const int row = lane + 32 * r;
       if (row < XR) {
-        const int comp = row / (N1 * N1), kj = row % (N1 * N1);
+        int comp, xk, xj;
+        S::x_row(row, comp, xk, xj);
+        const int kj = xk * N1 + xj;
 #pragma unroll
         for (int i = 0; i < N1; ++i) {
           const int packed = __ldg(cn + kj * N1 + i);
@@ -441,7 +443,8 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
       const int row = lane + 32 * r;
-      const int comp = row < XR ? row / (N1 * N1) : 0;
+      int comp = 0, xk, xj;
+      if (row < XR) S::x_row(row, comp, xk, xj);
       if (row >= XR) {
 #pragma unroll
         for (int i = 0; i < N1; ++i) { ck[r][i] = 0; v[r][i] = T(0); vu[r][i] = T(0); }
@@ -545,7 +548,8 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
     for (int r = 0; r < RPL; ++r) {
       const int row = lane + 32 * r;
       if (row < XR) {
-        const int comp = row / (N1 * N1);
+        int comp, xk, xj;
+        S::x_row(row, comp, xk, xj);
 #pragma unroll
         for (int i = 0; i < N1; ++i) {
           // distribute_local_to_global: constrained rows skipped
