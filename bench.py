@@ -423,6 +423,35 @@ def job_rate(world, n_dofs, steps, t_ms):
     return world * n_dofs * steps / (t_ms * 1e-3) / 1e9
 
 
+def profile_vcycle():
+    """One FP32 V-cycle of the 15^3 -> 30^3 Q2 hierarchy (tensor4, Chebyshev
+    degree 4, reference coarse solver) launched kernel by kernel between
+    cudaProfilerStart / Stop, so that a profiler started with profiling off
+    (ncu --profile-from-start off) records exactly that V-cycle."""
+    import torch
+    import lsmf
+    mesh = lsmf.Mesh("box", (15, 15, 15), 1, degree=2)
+    mesh.set_dirichlet([(4, 7)])
+    nc, nn, nd = mesh.info()
+    X, _, _ = mesh.arrays()
+    u = torch.tensor(smooth_field(X, 1).reshape(-1), device="cuda")
+    g = lsmf.GMG(mesh, "tensor4", 1, "fp32", degree=4)
+    g.set_material(np.ones(nc), NU)
+    g.set_graph(False)
+    g.setup(u)
+    b = torch.tensor(np.random.default_rng(0).uniform(-1, 1, nd), device="cuda")
+    b[torch.tensor(mesh.constraint_mask() == 1, device="cuda")] = 0
+    x = torch.empty_like(b)
+    g.vmult(x, b)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    g.vmult(x, b)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"profile_vcycle": "done", "coarse_level": g.level_info(0).tolist()}), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------- GPU (lsmf)
 def run_lsmf(args):
     import torch
@@ -634,11 +663,15 @@ def main():
     ap.add_argument("--newton-refinements", type=int, default=2)
     ap.add_argument("--cells", type=int, default=N_CELLS_1D, help="cells per direction (64 = the benchmark)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-gradient timing")
+    ap.add_argument("--profile-vcycle", action="store_true",
+                    help="only one FP32 V-cycle between cudaProfilerStart / Stop (for ncu --profile-from-start off)")
     ap.add_argument("--c5", action="store_true",
                     help="only the large configurations (128^3 Q2, 48^3 Q4 vmults; 128^3 inclusion Newton step)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_vcycle:
+        return profile_vcycle()
     if args.c5:
         print(json.dumps(c5_measurements()), flush=True)
         return 0
