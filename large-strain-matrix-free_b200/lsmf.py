@@ -108,6 +108,17 @@ SIGNATURES = {
 }
 
 
+def _release(obj, destroy_name):
+    """Destroy the handle of obj once.  The destroy function is taken from the
+    library object the handle came from (obj._L), so this also works while
+    the interpreter shuts down and module globals are already gone."""
+    h = getattr(obj, "h", None)
+    L = getattr(obj, "_L", None)
+    if h and L is not None:
+        obj.h = None
+        getattr(L, destroy_name)(h)
+
+
 def lib():
     """Load liblsmf.so (raises if it was not built)."""
     global _lib
@@ -153,14 +164,13 @@ class Mesh:
             d.coarse_active = self._mask.ctypes.data
         h = vp()
         check(lib().lsmf_mesh_create(ctypes.byref(d), ctypes.byref(h)))
+        self._L = lib()
         self.h = h
         self.degree = degree
         self.n_levels = lib().lsmf_mesh_n_levels(h)
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().lsmf_mesh_destroy(self.h)
-            self.h = None
+        _release(self, "lsmf_mesh_destroy")
 
     def info(self, level=-1):
         nc, nn, nd = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
@@ -197,14 +207,13 @@ class NeoHookOperator:
         h = vp()
         cach = CACHING[caching] if isinstance(caching, str) else int(caching)
         check(lib().lsmf_operator_create(mesh.h, level, cach, formulation, 1 if self.fp32 else 0, ctypes.byref(h)))
+        self._L = lib()
         self.h = h
         self.level = level
         self._u = None
 
     def clear(self):
-        if getattr(self, "h", None):
-            lib().lsmf_operator_destroy(self.h)
-            self.h = None
+        _release(self, "lsmf_operator_destroy")
 
     __del__ = clear
 
@@ -312,12 +321,11 @@ class GMG:
         d.coarse_chebyshev, d.coarse_accurate_eig = int(coarse_chebyshev), int(coarse_accurate_eig)
         h = vp()
         check(lib().lsmf_gmg_create(mesh.h, ctypes.byref(d), ctypes.byref(h)))
+        self._L = lib()
         self.h, self.mesh = h, mesh
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().lsmf_gmg_destroy(self.h)
-            self.h = None
+        _release(self, "lsmf_gmg_destroy")
 
     def set_material(self, mu_fine, nu):
         nc, _, _ = self.mesh.info(-1)
@@ -367,15 +375,14 @@ class Problem:
     def __init__(self, prm_text):
         h = vp()
         check(lib().lsmf_problem_create(prm_text.encode(), ctypes.byref(h)))
+        self._L = lib()
         self.h = h
         nc, nd, vol = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
         check(lib().lsmf_problem_info(h, ctypes.byref(nc), ctypes.byref(nd), ctypes.byref(vol)))
         self.n_cells, self.n_dofs, self.volume = nc.value, nd.value, vol.value
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().lsmf_problem_destroy(self.h)
-            self.h = None
+        _release(self, "lsmf_problem_destroy")
 
     def set_mu(self, mu_per_cell):
         mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu_per_cell, dtype=np.float64), (self.n_cells,)))
