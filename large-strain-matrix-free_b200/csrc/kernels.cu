@@ -820,7 +820,7 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask) {
   // loads, as do tensor2 and scalar (latency / FP64 bound)
   const bool ring_variant = VAR == VAR_TENSOR4 || VAR == VAR_TENSOR4_NS || VAR == VAR_SCALAR_REF;
   int stages = op->stages >= 0 ? op->stages : ((ring_variant && rec_bytes <= 24 * 1024) ? 1 : 0);
-  const int max_warps = op->max_warps > 0 ? op->max_warps : (VAR == VAR_TENSOR2 ? 8 : 4);
+  const int max_warps = op->max_warps > 0 ? op->max_warps : ((VAR == VAR_TENSOR2 && sizeof(T) == 8) ? 8 : 4);
   if (rec_bytes % 16 != 0) stages = 0;
   // fewer stages when the ring would leave fewer than 4 warps per block
   while (stages > 0 && warps_for_budget(wbytes(stages), 8, 220 * 1024) < 4) --stages;
