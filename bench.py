@@ -175,6 +175,15 @@ def cpu_vmult_rate(n_cells_1d, variant, fp32, steps, seed=1234):
     return m.n_dofs / t / 1e9, t, m.n_dofs
 
 
+def omp_binding():
+    """The OpenMP thread placement the CPU leg ran with."""
+    bind = os.environ.get("OMP_PROC_BIND")
+    places = os.environ.get("OMP_PLACES")
+    if not bind and not places:
+        return "no explicit pinning: OMP_PROC_BIND / OMP_PLACES unset"
+    return "OMP_PROC_BIND=%s OMP_PLACES=%s" % (bind, places)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -187,7 +196,8 @@ def run_reference(args):
             "config": {"workload": "tangent vmult, tensor4 caching, FP64, %d^3-cell Q2 unit cube" % args.cells,
                        "n_dofs": n_dofs, "parallelism": "OpenMP over host cores"},
             "cpu_baseline": {"value": rate, "unit": "GDoF/s", "cores": threads, "kind": "port",
-                             "sample": "%d vmults of the full %d^3 Q2 workload (median)" % (args.steps, args.cells)},
+                             "sample": "%d vmults of the full %d^3 Q2 workload (median), OpenMP over all %d host "
+                                       "threads (%s)" % (args.steps, args.cells, threads, omp_binding())},
             "e2e": {"value": rate, "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -628,7 +638,8 @@ def run_lsmf(args):
         threads = os.cpu_count() or 1
         rate, t, _ = cpu_vmult_rate(args.cells, "tensor4", False, 5)
         cpu = {"value": rate, "unit": "GDoF/s", "cores": threads, "kind": "port",
-               "sample": "5 vmults (median) of the full %d^3 Q2 tensor4 FP64 workload, OpenMP" % args.cells}
+               "sample": "5 vmults (median) of the full %d^3 Q2 tensor4 FP64 workload, OpenMP over all %d host "
+                         "threads (%s)" % (args.cells, threads, omp_binding())}
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 4), "unit": "GDoF/s", "n_gpus": world,
