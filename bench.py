@@ -433,14 +433,14 @@ def job_rate(world, n_dofs, steps, t_ms):
     return world * n_dofs * steps / (t_ms * 1e-3) / 1e9
 
 
-def profile_vcycle():
-    """One FP32 V-cycle of the 15^3 -> 30^3 Q2 hierarchy (tensor4, Chebyshev
-    degree 4, reference coarse solver) launched kernel by kernel between
-    cudaProfilerStart / Stop, so that a profiler started with profiling off
-    (ncu --profile-from-start off) records exactly that V-cycle."""
+def profile_vcycle(cells=15, refinements=1):
+    """One FP32 V-cycle of the cells^3 -> (cells 2^refinements)^3 Q2 hierarchy
+    (tensor4, Chebyshev degree 4, reference coarse solver) launched kernel by
+    kernel between cudaProfilerStart / Stop, so that a profiler started with
+    profiling off (ncu --profile-from-start off) records exactly that V-cycle."""
     import torch
     import lsmf
-    mesh = lsmf.Mesh("box", (15, 15, 15), 1, degree=2)
+    mesh = lsmf.Mesh("box", (cells,) * 3, refinements, degree=2)
     mesh.set_dirichlet([(4, 7)])
     nc, nn, nd = mesh.info()
     X, _, _ = mesh.arrays()
@@ -676,13 +676,15 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-gradient timing")
     ap.add_argument("--profile-vcycle", action="store_true",
                     help="only one FP32 V-cycle between cudaProfilerStart / Stop (for ncu --profile-from-start off)")
+    ap.add_argument("--profile-cells", type=int, default=15, help="coarse cells per direction of --profile-vcycle")
+    ap.add_argument("--profile-refinements", type=int, default=1, help="refinements of --profile-vcycle")
     ap.add_argument("--c5", action="store_true",
                     help="only the large configurations (128^3 Q2, 48^3 Q4 vmults; 128^3 inclusion Newton step)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.profile_vcycle:
-        return profile_vcycle()
+        return profile_vcycle(args.profile_cells, args.profile_refinements)
     if args.c5:
         print(json.dumps(c5_measurements()), flush=True)
         return 0
