@@ -768,23 +768,28 @@ template lsmf_status copy_indexed_async<double>(double *, const double *, const 
 
 template <typename T>
 lsmf_status cheb_zero_async(T *x, const T *b, const T *invd, double theta, size_t n, cudaStream_t st) {
-  cheb_zero_kernel<T><<<vec_grid(n), 256, 0, st>>>(x, b, invd, 1.0 / theta, n, vec_ok<T>({x, b, invd}, nullptr));
+  const int vec = vec_ok<T>({x, b, invd}, nullptr);
+  cheb_zero_kernel<T><<<vec_grid(vec ? (n + Vec16<T>::W - 1) / Vec16<T>::W : n), 256, 0, st>>>(x, b, invd, 1.0 / theta,
+                                                                                            n, vec);
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
 }
 template <typename T>
 lsmf_status cheb_first_async(T *x, T *xold, const T *b, T *r, const T *invd, const uint8_t *cmask, double theta,
                              size_t n, cudaStream_t st) {
-  cheb_first_kernel<T><<<vec_grid(n), 256, 0, st>>>(x, xold, b, r, invd, cmask, 1.0 / theta, n,
-                                                     vec_ok<T>({x, xold, b, r, invd}, cmask));
+  const int vec = vec_ok<T>({x, xold, b, r, invd}, cmask);
+  cheb_first_kernel<T><<<vec_grid(vec ? (n + Vec16<T>::W - 1) / Vec16<T>::W : n), 256, 0, st>>>(
+      x, xold, b, r, invd, cmask, 1.0 / theta, n, vec);
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
 }
 template <typename T>
 lsmf_status cheb_step_async(T *x, T *xold, const T *b, T *r, const T *invd, const uint8_t *cmask, double f1, double f2,
                             bool has_old, size_t n, cudaStream_t st) {
-  cheb_step_kernel<T><<<vec_grid(n), 256, 0, st>>>(x, xold, b, r, invd, cmask, f1, f2, has_old ? 1 : 0, n,
-                                                    vec_ok<T>({x, xold, b, r, invd}, cmask));
+  // one thread per 16-byte vector (the grid covers the vectors, not the values)
+  const int vec = vec_ok<T>({x, xold, b, r, invd}, cmask);
+  cheb_step_kernel<T><<<vec_grid(vec ? (n + Vec16<T>::W - 1) / Vec16<T>::W : n), 256, 0, st>>>(
+      x, xold, b, r, invd, cmask, f1, f2, has_old ? 1 : 0, n, vec);
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
 }
