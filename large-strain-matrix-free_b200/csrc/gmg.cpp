@@ -78,7 +78,9 @@ lsmf_status estimate_eigenvalues(lsmf_gmg *g, int l, int max_it, double &emin, d
   lsmf_op *op = GL.op;
   const size_t n = (size_t)op->L().n_dofs();
   cudaStream_t st = g->stream;
-  T *x = (T *)g->eig_vecs.ptr, *gg = x + n, *h = gg + n, *d = h + n;
+  // work vectors at 16-byte-aligned offsets (whole multiples of 4 values)
+  const size_t ns = (n + 3) / 4 * 4;
+  T *x = (T *)g->eig_vecs.ptr, *gg = x + ns, *h = gg + ns, *d = h + ns;
   const T *invd = (const T *)op->d_inv_diag.ptr;
   const uint8_t *cm = op->L().d_cmask.ptr;
   // start vector (i mod 11) - mean, made on the device; the mean of the
@@ -265,7 +267,8 @@ lsmf_status coarse_cg(lsmf_gmg *g) {
   cudaStream_t st = g->stream;
   const bool fp32 = sizeof(T) == 4;
   T *x = (T *)GL.x.ptr, *b = (T *)GL.b.ptr;
-  T *gg = (T *)g->eig_vecs.ptr, *h = gg + n, *d = h + n;
+  const size_t ns = (n + 3) / 4 * 4;  // 16-byte-aligned work vectors
+  T *gg = (T *)g->eig_vecs.ptr, *h = gg + ns, *d = h + ns;
   double *sc = g->sc.ptr, *part = g->partial.ptr;
   auto dot = [&](const T *a, const T *c, double &out) -> lsmf_status {
     LSMF_TRY(dot_async(a, c, fp32, n, part, sc, SC_TMP, st));
@@ -403,7 +406,7 @@ lsmf_status lsmf_gmg_create(lsmf_mesh *m, const lsmf_gmg_desc *desc, lsmf_gmg **
     s = lsmf_operator_create(m, l, (lsmf_caching)desc->caching, desc->formulation, desc->precision, &GL.op);
     if (s != LSMF_OK) break;
     const size_t n = (size_t)m->levels[l]->n_dofs() * g->elem();
-    nmax = std::max(nmax, n);
+    nmax = std::max(nmax, ((size_t)m->levels[l]->n_dofs() + 3) / 4 * 4 * g->elem());
     if ((s = GL.x.alloc(n)) != LSMF_OK || (s = GL.b.alloc(n)) != LSMF_OK || (s = GL.r.alloc(n)) != LSMF_OK ||
         (s = GL.xold.alloc(n)) != LSMF_OK || (s = GL.u.alloc(n)) != LSMF_OK)
       break;

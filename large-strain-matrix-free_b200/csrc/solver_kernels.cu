@@ -81,6 +81,45 @@ __global__ void cg_dir_kernel(double *d, const double *h, size_t n, const double
     d[i] = beta * d[i] - h[i];
 }
 
+// 16-byte vectors of level values (4 floats / 2 doubles) for the
+// bandwidth-bound element-wise kernels: one load instruction moves 16 bytes,
+// so a warp keeps 4x (2x) more bytes in flight than with scalar loads.  The
+// launchers use them only when every operand is 16-byte aligned (vec_ok).
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using type = float4;
+  static constexpr int W = 4;
+  __device__ static float get(const float4 &v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+  __device__ static void set(float4 &v, int k, float a) {
+    if (k == 0) v.x = a; else if (k == 1) v.y = a; else if (k == 2) v.z = a; else v.w = a;
+  }
+};
+template <>
+struct Vec16<double> {
+  using type = double2;
+  static constexpr int W = 2;
+  __device__ static double get(const double2 &v, int k) { return k == 0 ? v.x : v.y; }
+  __device__ static void set(double2 &v, int k, double a) {
+    if (k == 0) v.x = a; else v.y = a;
+  }
+};
+// true when every vector (and the mask, at W-byte granularity) allows the
+// 16-byte loads; sub-arrays of work buffers may not
+template <typename T>
+inline int vec_ok(std::initializer_list<const void *> ptrs, const uint8_t *cmask) {
+  for (const void *p : ptrs)
+    if ((uintptr_t)p % 16 != 0) return 0;
+  return (cmask == nullptr || (uintptr_t)cmask % Vec16<T>::W == 0) ? 1 : 0;
+}
+// W mask bytes starting at a multiple of W
+template <int W>
+__device__ __forceinline__ unsigned load_mask(const uint8_t *cm, size_t i) {
+  if (W == 4) return *(const unsigned *)(cm + i);
+  return *(const unsigned short *)(cm + i);
+}
+
 // history base of a replayed batch of eigenvalue-CG iterations
 __global__ void eig_advance_kernel(int *kbase, int by) { *kbase += by; }
 
@@ -106,12 +145,31 @@ __device__ __forceinline__ void block_partial(double s, double *partial) {
 }
 
 template <typename T>
-__global__ void eig_dh_kernel(const T *d, T *h, const uint8_t *cmask, size_t n, double *partial) {
+__global__ void eig_dh_kernel(const T *__restrict__ d, T *__restrict__ h, const uint8_t *__restrict__ cmask, size_t n,
+                              double *partial, int vec) {
+  using VT = Vec16<T>;
+  using V = typename VT::type;
+  constexpr int W = VT::W;
+  const size_t t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+  const size_t nv = vec ? n / W : 0;
   double s = 0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+  for (size_t v = t0; v < nv; v += st) {
+    const V dv = ((const V *)d)[v];
+    V hv = ((const V *)h)[v];
+    const unsigned cm = load_mask<W>(cmask, v * W);
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      T hi = VT::get(hv, k);
+      if ((cm >> (8 * k)) & 0xff) hi = hi + VT::get(dv, k);  // constrained row: identity
+      VT::set(hv, k, hi);
+      s += (double)VT::get(dv, k) * (double)hi;
+    }
+    if (cm) ((V *)h)[v] = hv;
+  }
+  for (size_t i = nv * W + t0; i < n; i += st) {
     T hi = h[i];
     if (cmask[i]) {
-      hi = hi + d[i];  // constrained row: identity
+      hi = hi + d[i];
       h[i] = hi;
     }
     s += (double)d[i] * (double)hi;
@@ -120,20 +178,40 @@ __global__ void eig_dh_kernel(const T *d, T *h, const uint8_t *cmask, size_t n, 
 }
 
 template <typename T>
-__global__ void eig_update_precond_kernel(T *g, T *h, const T *invd, size_t n, const double *sc, int gh_slot,
-                                          double *hist_alpha, int k, const int *kbase, double *partial_gg,
-                                          double *partial_gh) {
+__device__ __forceinline__ void eig_update_at(T &g, T &h, T invd, double alpha, double &s1, double &s2) {
+  const T gi = T((double)g + alpha * (double)h);
+  g = gi;
+  s1 += (double)gi * (double)gi;
+  const T hi = T(1) * invd * gi;  // Jacobi, omega = 1
+  h = hi;
+  s2 += (double)gi * (double)hi;
+}
+template <typename T>
+__global__ void eig_update_precond_kernel(T *__restrict__ g, T *__restrict__ h, const T *__restrict__ invd, size_t n,
+                                          const double *sc, int gh_slot, double *hist_alpha, int k,
+                                          const int *kbase, double *partial_gg, double *partial_gh, int vec) {
+  using VT = Vec16<T>;
+  using V = typename VT::type;
+  constexpr int W = VT::W;
   const double alpha = sc[gh_slot] / sc[SC_DH];
   if (blockIdx.x == 0 && threadIdx.x == 0) hist_alpha[(kbase ? *kbase : 0) + k] = alpha;
+  const size_t t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+  const size_t nv = vec ? n / W : 0;
   double s1 = 0, s2 = 0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const T gi = T((double)g[i] + alpha * (double)h[i]);
-    g[i] = gi;
-    s1 += (double)gi * (double)gi;
-    const T hi = T(1) * invd[i] * gi;  // Jacobi, omega = 1
-    h[i] = hi;
-    s2 += (double)gi * (double)hi;
+  for (size_t v = t0; v < nv; v += st) {
+    V gv = ((const V *)g)[v], hv = ((const V *)h)[v];
+    const V dv = ((const V *)invd)[v];
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+      T gq = VT::get(gv, q), hq = VT::get(hv, q);
+      eig_update_at<T>(gq, hq, VT::get(dv, q), alpha, s1, s2);
+      VT::set(gv, q, gq);
+      VT::set(hv, q, hq);
+    }
+    ((V *)g)[v] = gv;
+    ((V *)h)[v] = hv;
   }
+  for (size_t i = nv * W + t0; i < n; i += st) eig_update_at<T>(g[i], h[i], invd[i], alpha, s1, s2);
   block_partial(s1, partial_gg);
   block_partial(s2, partial_gh);
 }
@@ -162,11 +240,28 @@ __global__ void reduce2_final_kernel(const double *p1, const double *p2, int n, 
 }
 
 template <typename T>
-__global__ void eig_dir_clear_kernel(T *d, T *h, size_t n, const double *sc, int gh_new, int gh_old, double *hist_beta,
-                                     int k, const int *kbase) {
+__global__ void eig_dir_clear_kernel(T *__restrict__ d, T *__restrict__ h, size_t n, const double *sc, int gh_new,
+                                     int gh_old, double *hist_beta, int k, const int *kbase, int vec) {
+  using VT = Vec16<T>;
+  using V = typename VT::type;
+  constexpr int W = VT::W;
   const double beta = sc[gh_new] / sc[gh_old];
   if (blockIdx.x == 0 && threadIdx.x == 0) hist_beta[(kbase ? *kbase : 0) + k] = beta;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+  const size_t t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+  const size_t nv = vec ? n / W : 0;
+  for (size_t v = t0; v < nv; v += st) {
+    V dv = ((const V *)d)[v];
+    const V hv = ((const V *)h)[v];
+    V zero;
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+      VT::set(dv, q, T(beta * (double)VT::get(dv, q) - (double)VT::get(hv, q)));
+      VT::set(zero, q, T(0));
+    }
+    ((V *)d)[v] = dv;
+    ((V *)h)[v] = zero;
+  }
+  for (size_t i = nv * W + t0; i < n; i += st) {
     d[i] = T(beta * (double)d[i] - (double)h[i]);
     h[i] = T(0);
   }
@@ -217,44 +312,6 @@ __global__ void copy_indexed_kernel(T *dst, const T *src, const int *idx, int n)
 // x = D^-1 b / theta                                   (vmult, zero start)
 // x_old = x; x += D^-1 (b - r) / theta                 (step, first update)
 // x_new = x + f1 (x - x_old) + f2 D^-1 (b - r); x_old = x; x = x_new
-// 16-byte vectors of level values (4 floats / 2 doubles) for the
-// bandwidth-bound element-wise smoother kernels: one load instruction moves
-// 16 bytes, so a warp keeps 4x (2x) more bytes in flight than with scalar
-// loads.  Level vectors are separate allocations (256-byte aligned).
-template <typename T>
-struct Vec16;
-template <>
-struct Vec16<float> {
-  using type = float4;
-  static constexpr int W = 4;
-  __device__ static float get(const float4 &v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
-  __device__ static void set(float4 &v, int k, float a) {
-    if (k == 0) v.x = a; else if (k == 1) v.y = a; else if (k == 2) v.z = a; else v.w = a;
-  }
-};
-template <>
-struct Vec16<double> {
-  using type = double2;
-  static constexpr int W = 2;
-  __device__ static double get(const double2 &v, int k) { return k == 0 ? v.x : v.y; }
-  __device__ static void set(double2 &v, int k, double a) {
-    if (k == 0) v.x = a; else v.y = a;
-  }
-};
-// true when every vector (and the mask, at W-byte granularity) allows the
-// 16-byte loads; sub-arrays of work buffers may not
-template <typename T>
-inline int vec_ok(std::initializer_list<const void *> ptrs, const uint8_t *cmask) {
-  for (const void *p : ptrs)
-    if ((uintptr_t)p % 16 != 0) return 0;
-  return (cmask == nullptr || (uintptr_t)cmask % Vec16<T>::W == 0) ? 1 : 0;
-}
-// W mask bytes starting at a multiple of W
-template <int W>
-__device__ __forceinline__ unsigned load_mask(const uint8_t *cm, size_t i) {
-  if (W == 4) return *(const unsigned *)(cm + i);
-  return *(const unsigned short *)(cm + i);
-}
 
 template <typename T>
 __global__ void cheb_zero_kernel(T *__restrict__ x, const T *__restrict__ b, const T *__restrict__ invd,
@@ -640,7 +697,7 @@ template <typename T>
 lsmf_status eig_dh_async(const T *d, T *h, const uint8_t *cmask, size_t n, double *partial, double *sc,
                          cudaStream_t st) {
   const int gr = reduce_blocks();
-  eig_dh_kernel<T><<<gr, RED_THREADS, 0, st>>>(d, h, cmask, n, partial);
+  eig_dh_kernel<T><<<gr, RED_THREADS, 0, st>>>(d, h, cmask, n, partial, vec_ok<T>({d, h}, cmask));
   reduce_final_kernel<<<1, 1024, 0, st>>>(partial, gr, sc + SC_DH);
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
@@ -656,7 +713,7 @@ lsmf_status eig_update_precond_async(T *g, T *h, const T *invd, size_t n, double
                                      cudaStream_t st) {
   const int gr = reduce_blocks();
   eig_update_precond_kernel<T><<<gr, RED_THREADS, 0, st>>>(g, h, invd, n, sc, gh_slot, hist_alpha, k, kbase, partial,
-                                                           partial + gr);
+                                                           partial + gr, vec_ok<T>({g, h, invd}, nullptr));
   reduce2_final_kernel<<<1, 1024, 0, st>>>(partial, partial + gr, gr, hist_res2 + k, kbase, sc + gh_new);
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
@@ -669,7 +726,9 @@ template lsmf_status eig_update_precond_async<double>(double *, double *, const 
 template <typename T>
 lsmf_status eig_dir_clear_async(T *d, T *h, size_t n, const double *sc, int gh_new, int gh_old, double *hist_beta, int k,
                                 const int *kbase, cudaStream_t st) {
-  eig_dir_clear_kernel<T><<<vec_grid(n), 256, 0, st>>>(d, h, n, sc, gh_new, gh_old, hist_beta, k, kbase);
+  const int vec = vec_ok<T>({d, h}, nullptr);
+  eig_dir_clear_kernel<T><<<vec_grid(vec ? (n + Vec16<T>::W - 1) / Vec16<T>::W : n), 256, 0, st>>>(
+      d, h, n, sc, gh_new, gh_old, hist_beta, k, kbase, vec);
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
 }
