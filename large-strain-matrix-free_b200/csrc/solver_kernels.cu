@@ -428,14 +428,29 @@ __global__ void restrict_kernel(int n_coarse, const int *__restrict__ coarse_cn,
   double *in = (double *)smem_raw + warp * SZ, *s1 = in + 3 * NFB, *s2 = s1 + 3 * NF * NF * N1;
   for (int c = blockIdx.x * wpb + warp; c < n_coarse; c += gridDim.x * wpb) {
     const int *fn = fine_nodes + (size_t)c * NFB;
-    for (int l = lane; l < NFB; l += 32) {
-      const int node = fn[l];
-      const double w = weight[node];
+    // gather the fine block: all node ids of the lane first, then all
+    // weights and values, so every load of the lane is in flight at once
+    constexpr int NPL = (NFB + 31) / 32;
+    int node[NPL];
+#pragma unroll
+    for (int q = 0; q < NPL; ++q) node[q] = (lane + 32 * q < NFB) ? __ldg(fn + lane + 32 * q) : -1;
+    double w[NPL], bv[NPL][3], rv[NPL][3];
+#pragma unroll
+    for (int q = 0; q < NPL; ++q) {
+      if (node[q] < 0) continue;
+      w[q] = __ldg(weight + node[q]);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        const size_t d = 3 * (size_t)node + k;
-        in[k * NFB + l] = w * ((double)b[d] - (r ? (double)r[d] : 0.0));
+        const size_t d = 3 * (size_t)node[q] + k;
+        bv[q][k] = (double)b[d];
+        rv[q][k] = r ? (double)r[d] : 0.0;
       }
+    }
+#pragma unroll
+    for (int q = 0; q < NPL; ++q) {
+      if (node[q] < 0) continue;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) in[k * NFB + lane + 32 * q] = w[q] * (bv[q][k] - rv[q][k]);
     }
     __syncwarp();
     // z: s1[k][z][fy][fx] = sum_fz P[fz][z] in[k][fz][fy][fx]
@@ -478,7 +493,16 @@ __global__ void prolongate_kernel(int n_coarse, const int *__restrict__ coarse_c
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
   double *v = (double *)smem_raw + warp * SZ, *s1 = v + 3 * NCN, *s2 = s1 + 3 * N1 * N1 * NF;
+  constexpr int NPL = (NFB + 31) / 32;
   for (int c = blockIdx.x * wpb + warp; c < n_coarse; c += gridDim.x * wpb) {
+    // the lane's fine nodes and weights, loaded before the sweeps
+    const int *fn = fine_nodes + (size_t)c * NFB;
+    int node[NPL];
+    double w[NPL];
+#pragma unroll
+    for (int q = 0; q < NPL; ++q) node[q] = (lane + 32 * q < NFB) ? __ldg(fn + lane + 32 * q) : -1;
+#pragma unroll
+    for (int q = 0; q < NPL; ++q) w[q] = node[q] >= 0 ? __ldg(weight + node[q]) : 0.0;
     for (int it = lane; it < 3 * NCN; it += 32) {
       const int a = it % NCN, k = it / NCN;
       const int packed = coarse_cn[(size_t)c * NCN + a];
@@ -503,14 +527,17 @@ __global__ void prolongate_kernel(int n_coarse, const int *__restrict__ coarse_c
       s2[it] = s;
     }
     __syncwarp();
-    const int *fn = fine_nodes + (size_t)c * NFB;
-    for (int it = lane; it < 3 * NFB; it += 32) {
-      const int l = it % NFB, k = it / NFB, fyx = l % (NF * NF), fz = l / (NF * NF);
-      double s = 0;
 #pragma unroll
-      for (int z = 0; z < N1; ++z) s += pm.m[fz][z] * s2[(k * N1 + z) * NF * NF + fyx];
-      const int node = fn[l];
-      atomicAdd(fine + 3 * (size_t)node + k, T(weight[node] * s));
+    for (int q = 0; q < NPL; ++q) {
+      if (node[q] < 0) continue;
+      const int l = lane + 32 * q, fyx = l % (NF * NF), fz = l / (NF * NF);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        double s = 0;
+#pragma unroll
+        for (int z = 0; z < N1; ++z) s += pm.m[fz][z] * s2[(k * N1 + z) * NF * NF + fyx];
+        atomicAdd(fine + 3 * (size_t)node[q] + k, T(w[q] * s));
+      }
     }
     __syncwarp();
   }
