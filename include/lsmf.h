@@ -130,12 +130,13 @@ size_t lsmf_operator_memory_consumption(const lsmf_op *op);
 /* execution options (no reference counterpart; defaults are the fast path):
  * LSMF_OPT_BULK_PIPELINE: depth 1..3 of the shared-memory ring through which
  *   each warp streams its cell records with bulk copies; 0 = plain coalesced
- *   loads; -1 (default) = per-variant choice (tensor4: 1, others: 0).  The
+ *   loads; -1 (default) = measured choice: 1 for tensor4, tensor4_ns and
+ *   scalar_referential while a cell record fits in 24 KB, else 0.  The
  *   depth is reduced when the ring would not fit in shared memory.
  * LSMF_OPT_BASIC_KERNEL: 1 = the basic vmult kernel (per-warp shared-memory
  *   sweeps, plain loads); the stage mask of vmult always uses it.
  * LSMF_OPT_MAX_WARPS: cap on warps per block of the vmult kernel (1..8;
- *   0 = default: 8 for tensor2, 4 otherwise).
+ *   0 = default: 8 for FP64 tensor2, 4 otherwise).
  * A bounded device wait that runs out in the pipelined kernel is reported
  * as LSMF_ERR_TIMEOUT by the next synchronising call on the operator. */
 enum { LSMF_OPT_BULK_PIPELINE = 1, LSMF_OPT_BASIC_KERNEL = 2, LSMF_OPT_MAX_WARPS = 3 };
