@@ -200,8 +200,10 @@ lsmf_status lsmf_cg_solve(lsmf_op *fine, int precond, double omega, lsmf_gmg *gm
 
 /* ---- full problem: .prm driven load stepping (Solid::run) ---- */
 /* Parse a reference-format .prm text (ParameterHandler syntax, keys of
- * mf_elasticity.h:156-607) plus the additive keys documented in
- * INTEGRATION.md, build mesh, operators, GMG and loads. */
+ * mf_elasticity.h:156-607) plus the additive keys (Geometry: Type = Box,
+ * Box cells, Box lower corner, Box upper corner, Void spheres, Cook
+ * thickness; Linear solver: MF level precision, MF Chebyshev degree, MF
+ * Chebyshev smoothing range), build mesh, operators, GMG and loads. */
 lsmf_status lsmf_problem_create(const char *prm_text, lsmf_problem **out);
 /* Parse and check a .prm text without touching the device (undeclared keys,
  * bad values and unsupported options give LSMF_ERR_PRM / _UNSUPPORTED). */

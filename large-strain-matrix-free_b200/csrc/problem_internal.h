@@ -30,7 +30,10 @@ struct BCExpr {
 };
 
 // Keys of mf_elasticity.h:156-607 (defaults as declared there) plus the
-// additive keys documented in INTEGRATION.md.
+// additive keys without a reference counterpart: Geometry / Type = Box, Box
+// cells, Box lower / upper corner, Void spheres, Cook thickness; Linear
+// solver / MF level precision, MF Chebyshev degree, MF Chebyshev smoothing
+// range.
 struct ProblemParams {
   // Finite element system
   int degree = 2, quad_order = 3;
