@@ -438,7 +438,9 @@ lsmf_status lsmf_gmg_set_material(lsmf_gmg *g, const double *mu, double nu) {
 
 lsmf_status lsmf_gmg_setup(lsmf_gmg *g, const double *d_u) {
   if (!g || !d_u) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
-  drop_graph(g);
+  // the executable V-cycle graph is kept: the next vmult captures the new
+  // launch sequence and updates it in place
+  g->vstale = true;
   return g->desc.precision == LSMF_FP64 ? gmg_setup_impl<double>(g, d_u) : gmg_setup_impl<float>(g, d_u);
 }
 
@@ -462,10 +464,9 @@ lsmf_status lsmf_gmg_vmult(lsmf_gmg *g, double *dst, const double *src) {
   // the CG coarse solver reads scalars on the host, so that V-cycle is not
   // captured
   if (!g->use_graph || !g->desc.coarse_chebyshev) return run();
-  if (!g->vexec || g->vsrc != src || g->vdst != dst) {
+  if (!g->vexec || g->vstale || g->vsrc != src || g->vdst != dst) {
     // capture the V-cycle (a fixed sequence of launches once the Chebyshev
     // coefficients are known) on a private stream, then replay it
-    drop_graph(g);
     if (!g->cap_stream) LSMF_CUDA(cudaStreamCreateWithFlags(&g->cap_stream, cudaStreamNonBlocking));
     const cudaStream_t user = g->stream;
     lsmf_gmg_set_stream(g, g->cap_stream);
@@ -474,13 +475,35 @@ lsmf_status lsmf_gmg_vmult(lsmf_gmg *g, double *dst, const double *src) {
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(g->cap_stream, &graph);
     lsmf_gmg_set_stream(g, user);
-    if (s != LSMF_OK) { if (graph) cudaGraphDestroy(graph); return s; }
-    if (e != cudaSuccess) { set_error(std::string("V-cycle capture: ") + cudaGetErrorString(e)); return LSMF_ERR_CUDA; }
-    const cudaError_t ei = cudaGraphInstantiate(&g->vexec, graph, 0);
+    if (s != LSMF_OK) { if (graph) cudaGraphDestroy(graph); drop_graph(g); return s; }
+    if (e != cudaSuccess) { drop_graph(g); set_error(std::string("V-cycle capture: ") + cudaGetErrorString(e)); return LSMF_ERR_CUDA; }
+    // same launch sequence as the executable graph (same levels, degrees
+    // and kernels; new scalars and pointers): update it in place, which
+    // skips the instantiation (~2.4 ms for the ~1,600 nodes of a 762-step
+    // coarse solve); a changed sequence (another coarse degree) is
+    // instantiated anew
+    bool updated = false;
+    if (g->vexec) {
+      cudaGraphExecUpdateResultInfo info{};
+      updated = cudaGraphExecUpdate(g->vexec, graph, &info) == cudaSuccess;
+      if (!updated) {
+        (void)cudaGetLastError();  // the failed update is not sticky
+        drop_graph(g);
+      }
+    }
+    if (!updated) {
+      const cudaError_t ei = cudaGraphInstantiate(&g->vexec, graph, 0);
+      if (ei != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        g->vexec = nullptr;
+        set_error(std::string("V-cycle graph: ") + cudaGetErrorString(ei));
+        return LSMF_ERR_CUDA;
+      }
+    }
     cudaGraphDestroy(graph);
-    if (ei != cudaSuccess) { g->vexec = nullptr; set_error(std::string("V-cycle graph: ") + cudaGetErrorString(ei)); return LSMF_ERR_CUDA; }
     g->vsrc = src;
     g->vdst = dst;
+    g->vstale = false;
   }
   LSMF_CUDA(cudaGraphLaunch(g->vexec, g->stream));
   return LSMF_OK;

@@ -109,10 +109,13 @@ struct lsmf_gmg {
   lsmf::DevBuf<int> eig_kbase;   // history base of the replayed eigenvalue-CG batches
   cudaStream_t stream = 0;
   bool ready = false;
-  // the V-cycle replayed as one CUDA graph (captured after each set-up)
+  // the V-cycle replayed as one CUDA graph: captured again after each
+  // set-up (vstale) and applied to the executable graph in place when the
+  // launch sequence is unchanged
   bool use_graph = true;
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t vexec = nullptr;
+  bool vstale = true;
   const double *vsrc = nullptr;
   double *vdst = nullptr;
   size_t elem() const { return desc.precision == LSMF_FP64 ? 8 : 4; }

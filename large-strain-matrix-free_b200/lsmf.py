@@ -169,7 +169,7 @@ class Mesh:
         self.degree = degree
         self.n_levels = lib().lsmf_mesh_n_levels(h)
 
-    def __del__(self):
+    def __del__(self, _release=_release):  # bound now: module globals are gone at exit
         _release(self, "lsmf_mesh_destroy")
 
     def info(self, level=-1):
@@ -212,7 +212,7 @@ class NeoHookOperator:
         self.level = level
         self._u = None
 
-    def clear(self):
+    def clear(self, _release=_release):  # bound now: module globals are gone at exit
         _release(self, "lsmf_operator_destroy")
 
     __del__ = clear
@@ -324,7 +324,7 @@ class GMG:
         self._L = lib()
         self.h, self.mesh = h, mesh
 
-    def __del__(self):
+    def __del__(self, _release=_release):  # bound now: module globals are gone at exit
         _release(self, "lsmf_gmg_destroy")
 
     def set_material(self, mu_fine, nu):
@@ -381,7 +381,7 @@ class Problem:
         check(lib().lsmf_problem_info(h, ctypes.byref(nc), ctypes.byref(nd), ctypes.byref(vol)))
         self.n_cells, self.n_dofs, self.volume = nc.value, nd.value, vol.value
 
-    def __del__(self):
+    def __del__(self, _release=_release):  # bound now: module globals are gone at exit
         _release(self, "lsmf_problem_destroy")
 
     def set_mu(self, mu_per_cell):

@@ -86,6 +86,30 @@ def test_vcycle_large_coarse_level(precision, coarse_chebyshev):
     assert np.max(np.abs(got - want)) <= tol * np.max(np.abs(want))
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_vcycle_graph_follows_each_setup(precision):
+    # the executable V-cycle graph outlives a set-up and is updated in place
+    # from the next capture (or instantiated again when the coarse degree
+    # changes): after every set-up the replayed V-cycle is the new one
+    gm, mu, u, dirichlet, (lo, hi), rng = _problem("tensor4", 1, coarse=(6, 6, 6), nref=1)
+    g = lsmf.GMG(gm, "tensor4", 1, precision)
+    g.set_material(mu, 0.3)
+    src = rng.uniform(-1, 1, u.size)
+    src[gm.constraint_mask() == 1] = 0
+    dsrc = torch.tensor(src, device="cuda")
+    tol = 1e-10 if precision == "fp64" else 1e-4
+    for scale in (1.0, 1.0, 2.5, 0.5):
+        us = scale * u
+        g.setup(torch.tensor(us, device="cuda"))
+        ddst = torch.empty_like(dsrc)
+        g.vmult(ddst, dsrc)
+        og = O.GMG(O.GEOM_BOX, (6, 6, 6), 1, lo, hi, 1.0, 2, 3, "tensor4", 1, precision == "fp32", mu, 0.3,
+                   dirichlet, us)
+        assert g.level_info(0)[2] == og.level_info(0)[2]
+        want = og.vmult(src)
+        assert np.max(np.abs(ddst.cpu().numpy() - want)) <= tol * np.max(np.abs(want)), scale
+
+
 def test_vcycle_cook_geometry():
     gm, mu, u, dirichlet, (lo, hi), rng = _problem("tensor4", 1, coarse=(2, 2, 1), nref=1, geometry="cook")
     og = O.GMG(O.GEOM_COOK, (2, 2, 1), 1, lo, hi, 1.0, 2, 3, "tensor4", 1, False, mu, 0.3, dirichlet, u)
