@@ -178,8 +178,10 @@ lsmf_status lsmf_gmg_level_info(const lsmf_gmg *g, int level, double *out6);
 /* CUDA stream of every level operation (cudaStream_t) */
 lsmf_status lsmf_gmg_set_stream(lsmf_gmg *g, void *stream);
 /* options: LSMF_GMG_OPT_GRAPH = 1 (default) replays the V-cycle as one CUDA
- * graph captured after each set-up (for a given pair of vmult buffers);
- * 0 launches the kernels one by one. */
+ * graph (for a given pair of vmult buffers); the first vmult after a set-up
+ * captures the new launch sequence and updates the executable graph in
+ * place, or instantiates it again when the sequence changed (another coarse
+ * Chebyshev degree).  0 launches the kernels one by one. */
 enum { LSMF_GMG_OPT_GRAPH = 1 };
 lsmf_status lsmf_gmg_set_option(lsmf_gmg *g, int option, int value);
 

@@ -136,6 +136,19 @@ __device__ __forceinline__ void decode_row(int row, int idx[3]) {
   idx[I2] = row / (D[I0] * D[I1]);
 }
 
+// Visit the rows lane, lane + 32, ... of a sweep with NR rows: f(row, act).
+// CLAMP with NR <= 32: every lane takes one row, lanes past the end repeat
+// the last row (act = false: they compute, but store nothing), so the sweep
+// has no divergent branch.
+template <int NR, bool CLAMP, typename F>
+__device__ __forceinline__ void rows_of_lane(int lane, F &&f) {
+  if constexpr (CLAMP && NR <= 32) {
+    f(lane < NR ? lane : NR - 1, lane < NR);
+  } else {
+    for (int row = lane; row < NR; row += 32) f(row, true);
+  }
+}
+
 // Sum factorisation with one 1D line per lane ("row" sweeps).  Each sweep
 // maps lane -> row of the tensor it produces and unrolls the 1D contraction
 // completely; shared memory only carries the transposes between sweeps.
@@ -143,7 +156,11 @@ __device__ __forceinline__ void decode_row(int row, int idx[3]) {
 //              per-point gradient registers
 //   integrate: per-point H -> Z (z) -> Y (y) -> per-row nodal values (x)
 // Slab layout (elements of T): [9*NQ points][2*NA][3*NB].
-template <int P, int Q, typename T>
+// CLAMP: with at most 32 rows / points per sweep, the lanes past the end
+// repeat the last row or point and only their stores are skipped (no
+// divergent branches; measured faster for the scalar variants, whose
+// kernels carry the most registers, and slower for tensor2)
+template <int P, int Q, typename T, bool CLAMP = false>
 struct SFR {
   using LY = SFRLayout<P, (int)sizeof(T)>;
   static constexpr int N1 = P + 1, NN = N1 * N1 * N1, NQ = Q * Q * Q;
@@ -178,10 +195,11 @@ struct SFR {
     T *Pt = slab, *A = slab + SZP, *B = A + 2 * NA;
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
-      const int row = lane + 32 * r;
-      if (row < XR) {
+      const int row0 = lane + 32 * r;
+      if ((CLAMP && XR <= 32) || row0 < XR) {
+        const bool act = row0 < XR;
         int c, k, j;
-        x_row(row, c, k, j);
+        x_row(act ? row0 : XR - 1, c, k, j);
 #pragma unroll
         for (int qx = 0; qx < Q; ++qx) {
           T s0 = 0, s1 = 0;
@@ -190,13 +208,15 @@ struct SFR {
             s0 += t.N[qx][i] * v[r][i];
             s1 += t.D[qx][i] * v[r][i];
           }
-          A[a_at(c, k, j, qx)] = s0;
-          A[NA + a_at(c, k, j, qx)] = s1;
+          if (act) {
+            A[a_at(c, k, j, qx)] = s0;
+            A[NA + a_at(c, k, j, qx)] = s1;
+          }
         }
       }
     }
     __syncwarp();
-    for (int row = lane; row < YR; row += 32) {
+    rows_of_lane<YR, CLAMP>(lane, [&](int row, bool act) {
       int ix[3];
       decode_row<LY::Y0, LY::Y1, LY::Y2, 3, N1, Q>(row, ix);
       const int c = ix[0], k = ix[1], qx = ix[2];
@@ -216,13 +236,15 @@ struct SFR {
           s10 += t.N[qy][j] * a1[j];
         }
         const int b = b_at(c, k, qy, qx);
-        B[b] = s00;
-        B[NB + b] = s01;
-        B[2 * NB + b] = s10;
+        if (act) {
+          B[b] = s00;
+          B[NB + b] = s01;
+          B[2 * NB + b] = s10;
+        }
       }
-    }
+    });
     __syncwarp();
-    for (int row = lane; row < ZR; row += 32) {
+    rows_of_lane<ZR, CLAMP>(lane, [&](int row, bool act) {
       int ix[3];
       decode_row<LY::Z0, LY::Z1, LY::Z2, 3, Q, Q>(row, ix);
       const int qyx = ix[1] * Q + ix[2], c = ix[0];
@@ -244,11 +266,13 @@ struct SFR {
           gz += t.D[qz][k] * b00[k];
         }
         const int q = qz * Q * Q + qyx;
-        Pt[(c * 3 + 0) * NQP + q] = gx;
-        Pt[(c * 3 + 1) * NQP + q] = gy;
-        Pt[(c * 3 + 2) * NQP + q] = gz;
+        if (act) {
+          Pt[(c * 3 + 0) * NQP + q] = gx;
+          Pt[(c * 3 + 1) * NQP + q] = gy;
+          Pt[(c * 3 + 2) * NQP + q] = gz;
+        }
       }
-    }
+    });
     __syncwarp();
   }
 
@@ -259,8 +283,9 @@ struct SFR {
     const T *Pt = slab;
 #pragma unroll
     for (int l = 0; l < QPL; ++l) {
-      const int q = lane + 32 * l;
-      if (q < NQ) {
+      // lanes past the last point read the last point (no divergent branch)
+      const int q = (CLAMP && NQ <= 32) ? (lane < NQ ? lane : NQ - 1) : lane + 32 * l;
+      if ((CLAMP && NQ <= 32) || q < NQ) {
 #pragma unroll
         for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -291,7 +316,7 @@ struct SFR {
   static __device__ __forceinline__ void integrate_pt(const TabT<P, Q, T> &t, T *slab, int lane, T out[RPL][N1]) {
     T *Pt = slab, *Y = slab + SZP, *Z = Y + 2 * NA;
     __syncwarp();
-    for (int row = lane; row < ZR; row += 32) {
+    rows_of_lane<ZR, CLAMP>(lane, [&](int row, bool act) {
       int ix[3];
       decode_row<LY::Z0, LY::Z1, LY::Z2, 3, Q, Q>(row, ix);
       const int qyx = ix[1] * Q + ix[2], c = ix[0];
@@ -313,13 +338,15 @@ struct SFR {
           sz += t.D[qz][k] * hz[qz];
         }
         const int z = b_at(c, k, ix[1], ix[2]);
-        Z[z] = sx;
-        Z[NB + z] = sy;
-        Z[2 * NB + z] = sz;
+        if (act) {
+          Z[z] = sx;
+          Z[NB + z] = sy;
+          Z[2 * NB + z] = sz;
+        }
       }
-    }
+    });
     __syncwarp();
-    for (int row = lane; row < YR; row += 32) {
+    rows_of_lane<YR, CLAMP>(lane, [&](int row, bool act) {
       int ix[3];
       decode_row<LY::Y0, LY::Y1, LY::Y2, 3, N1, Q>(row, ix);
       const int c = ix[0], k = ix[1], qx = ix[2];
@@ -340,17 +367,20 @@ struct SFR {
           so += t.D[qy][j] * zy[qy] + t.N[qy][j] * zz[qy];
         }
         const int y = a_at(c, k, j, qx);
-        Y[y] = sx;
-        Y[NA + y] = so;
+        if (act) {
+          Y[y] = sx;
+          Y[NA + y] = so;
+        }
       }
-    }
+    });
     __syncwarp();
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
-      const int row = lane + 32 * r;
-      if (row < XR) {
+      const int row0 = lane + 32 * r;
+      // lanes past the last row compute the last row (their out is unused)
+      if ((CLAMP && XR <= 32) || row0 < XR) {
         int c, k, j;
-        x_row(row, c, k, j);
+        x_row(row0 < XR ? row0 : XR - 1, c, k, j);
         T yx[Q], yo[Q];
 #pragma unroll
         for (int qx = 0; qx < Q; ++qx) {

@@ -367,9 +367,13 @@ __global__ void __launch_bounds__(256) apply_kernel(KArgs<T> a, Tab<P, Q> tab) {
 // STAGES == 0 the record is read with plain coalesced loads.
 template <int P, int Q, typename T, int VAR, int STAGES>
 __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, T> tab) {
-  using S = SFR<P, Q, T>;
-  constexpr int N1 = P + 1, NN = S::NN, NQ = S::NQ, QPL = S::QPL, RPL = S::RPL, XR = S::XR;
   constexpr bool SCALAR = (VAR == VAR_SCALAR_F0 || VAR == VAR_SCALAR_F1);
+  // branch-free sweeps and point loop for the scalar variants (48^3 / 64^3
+  // Q2: scalar -7 % FP64 / -10 % FP32, scalar_referential -4 % / -17 %;
+  // tensor2 +4-6 % and tensor4 +1 %, so those keep the divergent form)
+  constexpr bool CLAMP = SCALAR || VAR == VAR_SCALAR_REF;
+  using S = SFR<P, Q, T, CLAMP>;
+  constexpr int N1 = P + 1, NN = S::NN, NQ = S::NQ, QPL = S::QPL, RPL = S::RPL, XR = S::XR;
   // several points per lane (Q^3 > 32): the gradients stay in the slab's
   // point block and each point is read, transformed and overwritten there
   // in turn, instead of holding 2 x 9 x QPL values in registers (the FP64 Q4
@@ -418,9 +422,10 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
       const int row = lane + 32 * r;
-      if (row < XR) {
+      // (CLAMP) lanes past the last row load the last row again
+      if ((CLAMP && XR <= 32) || row < XR) {
         int comp, xk, xj;
-        S::x_row(row, comp, xk, xj);
+        S::x_row(row < XR ? row : XR - 1, comp, xk, xj);
         const int kj = xk * N1 + xj;
 #pragma unroll
         for (int i = 0; i < N1; ++i) {
@@ -444,8 +449,10 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
     for (int r = 0; r < RPL; ++r) {
       const int row = lane + 32 * r;
       int comp = 0, xk, xj;
-      if (row < XR) S::x_row(row, comp, xk, xj);
-      if (row >= XR) {
+      // (CLAMP: the lanes past the last row carry a copy of it; the sweeps
+      // store nothing from them and the scatter skips them)
+      if ((CLAMP && XR <= 32) || row < XR) S::x_row(row < XR ? row : XR - 1, comp, xk, xj);
+      if (!(CLAMP && XR <= 32) && row >= XR) {
 #pragma unroll
         for (int i = 0; i < N1; ++i) { ck[r][i] = 0; v[r][i] = T(0); vu[r][i] = T(0); }
         continue;
@@ -481,12 +488,14 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
     T H[QPL][3][3];
 #pragma unroll(PT_SMEM ? 1 : QPL)
     for (int l = 0; l < QPL; ++l) {
-      const int q = lane + 32 * l;
+      // (CLAMP: the lanes past the last point repeat it; their H is never
+      // stored)
+      const int q = (CLAMP && NQ <= 32) ? (lane < NQ ? lane : NQ - 1) : lane + 32 * l;
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int e = 0; e < 3; ++e) H[l][c][e] = T(0);
-      if (q >= NQ) continue;
+      if (!(CLAMP && NQ <= 32) && q >= NQ) continue;
       const T *r = rec + q;
       T Ji[3][3];
 #pragma unroll
