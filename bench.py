@@ -225,24 +225,22 @@ def voids_prm(level_precision, cells=15, refinements=2, degree=4):
         "subsection Time", "  set End time = 0.1", "  set Time step size = 0.1", "end", ""])
 
 
-def newton_step_times(cells=15, refinements=2, repeats=3, device_index=0):
-    """Run one load step of the voids problem with FP32 and with FP64 level
-    operators; return per-form Newton-step times (device-timed residual +
-    set-up + CG; median of `repeats` solves, the two forms alternating so
-    that neither always runs first after other work) and the relative
-    difference of the two solutions."""
+def compare_level_precisions(prm_of, repeats=3, device_index=0, mu=None):
+    """Solve the first load step of the problem prm_of(level_precision) with
+    FP32 and with FP64 GMG levels: one untimed solve per form (the first
+    solve of a problem also instantiates its V-cycle and eigenvalue-CG
+    graphs and allocates work buffers, which later load steps reuse), then
+    `repeats` device-timed solves per form, the two forms alternating so that
+    neither always runs first after other work.  Returns per-form medians of
+    the time per Newton iteration (residual + set-up + CG), the clocks seen,
+    the speed-up and the relative difference of the two solutions."""
     import lsmf
-    out = {}
-    sols = {}
-    # warm-up on a small mesh so that module loading and first-launch costs
-    # are not charged to the first form
-    for prec in ("float", "double"):
-        lsmf.Problem(voids_prm(prec, 4, 1)).run()
     forms = (("fp32_gmg", "float"), ("fp64_gmg", "double"))
-    pbs = {form: lsmf.Problem(voids_prm(prec, cells, refinements)) for form, prec in forms}
-    # one untimed full-size solve per form: the first solve of a problem
-    # also instantiates its V-cycle and eigenvalue-CG graphs and allocates
-    # work buffers, which later load steps reuse
+    pbs = {}
+    for form, prec in forms:
+        pbs[form] = lsmf.Problem(prm_of(prec))
+        if mu is not None:
+            pbs[form].set_mu(mu)
     for form, _ in forms:
         pbs[form].run()
     runs = {form: [] for form, _ in forms}
@@ -255,6 +253,7 @@ def newton_step_times(cells=15, refinements=2, repeats=3, device_index=0):
             total = res["time_residual"] + res["time_setup"] + res["time_solve"]
             runs[form].append((total / max(1, st["newton_iterations"]), res, st))
     clocks = sampler.stop()
+    out, sols = {}, {}
     for form, _ in forms:
         rs = sorted(runs[form], key=lambda r: r[0])
         per_step, res, st = rs[len(rs) // 2]
@@ -269,6 +268,18 @@ def newton_step_times(cells=15, refinements=2, repeats=3, device_index=0):
     a, b = sols["fp32_gmg"], sols["fp64_gmg"]
     out["speedup_fp32_over_fp64"] = round(out["fp64_gmg"]["s_per_newton_step"] / out["fp32_gmg"]["s_per_newton_step"], 3)
     out["solution_rel_diff"] = float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+    return out
+
+
+def newton_step_times(cells=15, refinements=2, repeats=3, device_index=0):
+    """One load step of the voids problem with FP32 and with FP64 level
+    operators (compare_level_precisions)."""
+    import lsmf
+    # warm-up on a small mesh so that module loading and first-launch costs
+    # are not charged to the first form
+    for prec in ("float", "double"):
+        lsmf.Problem(voids_prm(prec, 4, 1)).run()
+    out = compare_level_precisions(lambda prec: voids_prm(prec, cells, refinements), repeats, device_index)
     out["workload"] = "voids: 60^3 Q2 cube minus 16 spheres r=0.08, tensor4, first load step, CG to 1e-8"
     return out
 
@@ -398,32 +409,12 @@ def c5_measurements(repeats=3):
     """The large configurations: vmult rates at 128^3 Q2 and 48^3 Q4
     (tensor4, FP64 and FP32), and one Newton iteration of the 128^3 Q2
     inclusion problem with FP32 and with FP64 GMG levels."""
-    import lsmf
     out = {"vmult": {}}
     for cells, degree in ((128, 2), (48, 4)):
         for prec in ("fp64", "fp32"):
             out["vmult"]["%d^3_Q%d_tensor4_%s" % (cells, degree, prec)] = vmult_rate(cells, degree, "tensor4", prec)
     mu, frac = inclusion_mu()
-    sols = {}
-    for form, prec in (("fp32_gmg", "float"), ("fp64_gmg", "double")):
-        pb = lsmf.Problem(inclusions_prm(prec))
-        pb.set_mu(mu)
-        runs = []
-        for _ in range(repeats):
-            res = pb.run()
-            st = res["steps"][0]
-            total = res["time_residual"] + res["time_setup"] + res["time_solve"]
-            runs.append((total / max(1, st["newton_iterations"]), res, st))
-        runs.sort(key=lambda r: r[0])
-        per_step, res, st = runs[len(runs) // 2]
-        out[form] = {"n_dofs": pb.n_dofs, "newton_iterations": st["newton_iterations"],
-                     "cg_iterations": st["cg_iterations"], "s_per_newton_step": round(per_step, 4),
-                     "setup_s": round(res["time_setup"], 4), "solve_s": round(res["time_solve"], 4)}
-        sols[form] = pb.solution()
-        del pb
-    a, b = sols["fp32_gmg"], sols["fp64_gmg"]
-    out["speedup_fp32_over_fp64"] = round(out["fp64_gmg"]["s_per_newton_step"] / out["fp32_gmg"]["s_per_newton_step"], 3)
-    out["solution_rel_diff"] = float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+    out.update(compare_level_precisions(inclusions_prm, repeats, int(os.environ.get("LOCAL_RANK", "0")), mu))
     out["workload"] = ("inclusions: 128^3 Q2 unit cube, mu = 10 in 32 seeded spheres (%.1f %% of the cells), "
                        "tensor4, first load step, CG to 1e-8" % (100 * frac))
     return out
