@@ -161,39 +161,77 @@ lsmf_status estimate_eigenvalues(lsmf_gmg *g, int l, int max_it, double &emin, d
       cudaGraphDestroy(graph);
       if (ei != cudaSuccess) { set_error(std::string("eigenvalue CG graph: ") + cudaGetErrorString(ei)); return LSMF_ERR_CUDA; }
     }
-    int k = 0;
-    bool done = false;
+    // Batches are pipelined: batch i + 1 is launched before the host reads
+    // the history of batch i (pinned copies + an event), so the GPU does not
+    // wait for the host's convergence check.  A batch launched after the
+    // converged one only writes history past the cut and scratch vectors.
+    if (!g->eig_pinned && cudaMallocHost((void **)&g->eig_pinned, 2 * 3 * 8 * sizeof(double)) != cudaSuccess) {
+      g->eig_pinned = nullptr;
+      if (bexec) cudaGraphExecDestroy(bexec);
+      set_error("cudaMallocHost of the eigenvalue-CG history copies failed");
+      return LSMF_ERR_ALLOC;
+    }
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int slot_n[2] = {0, 0};
+    bool slot_busy[2] = {false, false};
     lsmf_status status = LSMF_OK;
-    std::vector<double> A(8), Bt(8), Rs(8);
-    double prev_beta = 0, prev_alpha = 0;
-    while (!done && k < max_it && status == LSMF_OK) {
+    for (int s = 0; s < 2 && status == LSMF_OK; ++s)
+      if (cudaEventCreateWithFlags(&ev[s], cudaEventDisableTiming) != cudaSuccess) {
+        set_error("cudaEventCreate failed");
+        status = LSMF_ERR_CUDA;
+      }
+    int k = 0;  // first iteration not launched yet
+    // launch the batch k .. k + n - 1 and the copies of its history into slot s
+    auto issue = [&](int s) -> lsmf_status {
       const int batch = std::min(8, max_it - k);
       if (bexec && batch == 8) {
         // the replayed batch writes history k .. k + 7 (its base is k)
         const cudaError_t e = cudaGraphLaunch(bexec, st);
-        if (e != cudaSuccess) { set_error(std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); status = LSMF_ERR_CUDA; break; }
-      } else if ((status = batch_launch(k, batch, nullptr)) != LSMF_OK) {
-        break;
+        if (e != cudaSuccess) { set_error(std::string("cudaGraphLaunch: ") + cudaGetErrorString(e)); return LSMF_ERR_CUDA; }
+      } else {
+        LSMF_TRY(batch_launch(k, batch, nullptr));
       }
+      double *P = g->eig_pinned + s * 24;
+      cudaError_t e = cudaMemcpyAsync(P, ha + k, batch * sizeof(double), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(P + 8, hb + k, batch * sizeof(double), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(P + 16, hr + k, batch * sizeof(double), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaEventRecord(ev[s], st);
+      if (e != cudaSuccess) { set_error(std::string("eigenvalue CG history: ") + cudaGetErrorString(e)); return LSMF_ERR_CUDA; }
+      slot_n[s] = batch;
+      slot_busy[s] = true;
       k += batch;
-      cudaError_t e = cudaMemcpyAsync(A.data(), ha + (k - batch), batch * sizeof(double), cudaMemcpyDeviceToHost, st);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(Bt.data(), hb + (k - batch), batch * sizeof(double), cudaMemcpyDeviceToHost, st);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(Rs.data(), hr + (k - batch), batch * sizeof(double), cudaMemcpyDeviceToHost, st);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      return LSMF_OK;
+    };
+    bool done = false;
+    double prev_beta = 0, prev_alpha = 0;
+    int cur = 0;
+    if (status == LSMF_OK && max_it > 0) status = issue(cur);
+    while (status == LSMF_OK && !done && slot_busy[cur]) {
+      if (k < max_it && (status = issue(cur ^ 1)) != LSMF_OK) break;
+      const cudaError_t e = cudaEventSynchronize(ev[cur]);
+      slot_busy[cur] = false;
       if (e != cudaSuccess) { set_error(std::string("eigenvalue CG history: ") + cudaGetErrorString(e)); status = LSMF_ERR_CUDA; break; }
-      for (int j = 0; j < batch && !done; ++j) {
+      const double *P = g->eig_pinned + cur * 24;
+      for (int j = 0; j < slot_n[cur] && !done; ++j) {
         ++its;
-        const double alpha = A[j];
+        const double alpha = P[j];
         if (its > 1) {
           dT.push_back(1.0 / alpha + prev_beta / prev_alpha);
           oT.push_back(std::sqrt(prev_beta) / prev_alpha);
         } else {
           dT.push_back(1.0 / alpha);
         }
-        if (std::sqrt(Rs[j]) <= tol || its >= max_it) done = true;
-        prev_beta = Bt[j];
+        if (std::sqrt(P[16 + j]) <= tol || its >= max_it) done = true;
+        prev_beta = P[8 + j];
         prev_alpha = alpha;
       }
+      cur ^= 1;
+    }
+    // a batch launched past the converged one may still be copying into
+    // the pinned slots: wait for it before they can be reused
+    for (int s = 0; s < 2; ++s) {
+      if (slot_busy[s]) cudaEventSynchronize(ev[s]);
+      if (ev[s]) cudaEventDestroy(ev[s]);
     }
     if (bexec) cudaGraphExecDestroy(bexec);
     if (status != LSMF_OK) return status;
@@ -380,6 +418,7 @@ static void drop_graph(lsmf_gmg *g) {
 
 lsmf_gmg::~lsmf_gmg() {
   drop_graph(this);
+  if (eig_pinned) cudaFreeHost(eig_pinned);
   if (cap_stream) cudaStreamDestroy(cap_stream);
   for (auto &GL : levels) lsmf_operator_destroy(GL.op);
 }

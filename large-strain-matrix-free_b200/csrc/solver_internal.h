@@ -107,6 +107,9 @@ struct lsmf_gmg {
   lsmf::DevBuf<char> eig_vecs;  // scratch for the eigenvalue CG (4 level vectors)
   lsmf::DevBuf<double> eig_hist; // alpha / beta / residual history of the eigenvalue CG
   lsmf::DevBuf<int> eig_kbase;   // history base of the replayed eigenvalue-CG batches
+  // pinned host copies of two batches of alpha / beta / residual history
+  // (2 slots x 3 x 8 doubles), read while the next batch runs
+  double *eig_pinned = nullptr;
   cudaStream_t stream = 0;
   bool ready = false;
   // the V-cycle replayed as one CUDA graph: captured again after each
