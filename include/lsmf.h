@@ -124,9 +124,16 @@ lsmf_status lsmf_operator_compute_diagonal(lsmf_op *op);
 lsmf_status lsmf_operator_get_diagonal(lsmf_op *op, const void **d_diag, const void **d_inv_diag);
 /* precondition_Jacobi(): dst = omega * D^-1 src (mf_nh_operator.h:348-360) */
 lsmf_status lsmf_operator_precondition_jacobi(lsmf_op *op, void *d_dst, const void *d_src, double omega);
-/* m(), n(), memory_consumption() (mf_nh_operator.h:300-392) */
+/* m(), n(), memory_consumption() (mf_nh_operator.h:300-392): rows and
+ * columns (n_dofs); bytes of the cache tables plus the index map and node
+ * coordinates (the MatrixFree data), diagonals excluded like the reference */
 int lsmf_operator_m(const lsmf_op *op);
+int lsmf_operator_n(const lsmf_op *op);
 size_t lsmf_operator_memory_consumption(const lsmf_op *op);
+/* el(row, col) (mf_nh_operator.h:1562-1571): the diagonal entry; needs
+ * compute_diagonal(); row != col gives LSMF_ERR_UNSUPPORTED (the reference's
+ * ExcNotImplemented).  Synchronous (one value copied to the host). */
+lsmf_status lsmf_operator_el(lsmf_op *op, int row, int col, double *value);
 /* execution options (no reference counterpart; defaults are the fast path):
  * LSMF_OPT_BULK_PIPELINE: depth 1..3 of the shared-memory ring through which
  *   each warp streams its cell records with bulk copies; 0 = plain coalesced
@@ -137,10 +144,29 @@ size_t lsmf_operator_memory_consumption(const lsmf_op *op);
  *   sweeps, plain loads); the stage mask of vmult always uses it.
  * LSMF_OPT_MAX_WARPS: cap on warps per block of the vmult kernel (1..8;
  *   0 = default: 8 for FP64 tensor2, 4 otherwise).
+ * LSMF_OPT_WAIT_TRIES: bound of the pipelined kernel's wait for a cell
+ *   record (mbarrier try_wait calls; -1 = default 2^22, seconds).  A wait
+ *   that runs out sets the operator's device error word, lets every copy
+ *   the warp still has in flight land (default bound) and ends the warp;
+ *   0 makes every wait run out at once (for tests of that path).
+ * LSMF_OPT_SCATTER: 0 (default) = the cell loop adds its contributions
+ *   with atomics (summation order varies run to run); 1 = colour8: the
+ *   cells are processed in the 8 parity colours of the structured lattice,
+ *   one launch per colour, so that no two cells of a launch share a node
+ *   and the sums are formed in a fixed order without atomics
+ *   (bit-reproducible vmult, for parity and debugging).
  * A bounded device wait that runs out in the pipelined kernel is reported
- * as LSMF_ERR_TIMEOUT by the next synchronising call on the operator. */
-enum { LSMF_OPT_BULK_PIPELINE = 1, LSMF_OPT_BASIC_KERNEL = 2, LSMF_OPT_MAX_WARPS = 3 };
+ * as LSMF_ERR_TIMEOUT by lsmf_operator_sync, lsmf_cg_solve and the GMG
+ * set-up (the next synchronising call on the operator). */
+enum { LSMF_OPT_BULK_PIPELINE = 1, LSMF_OPT_BASIC_KERNEL = 2, LSMF_OPT_MAX_WARPS = 3, LSMF_OPT_WAIT_TRIES = 4,
+       LSMF_OPT_SCATTER = 5 };
+enum { LSMF_SCATTER_ATOMIC = 0, LSMF_SCATTER_COLOUR8 = 1 };
 lsmf_status lsmf_operator_set_option(lsmf_op *op, int option, int value);
+/* Wait for the operator's stream and report a device error its kernels
+ * recorded since the last report (LSMF_ERR_TIMEOUT for a bounded wait that
+ * ran out; the word is cleared once reported).  No reference counterpart:
+ * deal.II's vmult is synchronous and has no device waits. */
+lsmf_status lsmf_operator_sync(lsmf_op *op);
 /* the CUDA stream every operator call is ordered on (cudaStream_t) */
 lsmf_status lsmf_operator_set_stream(lsmf_op *op, void *stream);
 /* copy a cache table to the host for checking: which = 0 scalar / c1,
@@ -181,8 +207,11 @@ lsmf_status lsmf_gmg_set_stream(lsmf_gmg *g, void *stream);
  * graph (for a given pair of vmult buffers); the first vmult after a set-up
  * captures the new launch sequence and updates the executable graph in
  * place, or instantiates it again when the sequence changed (another coarse
- * Chebyshev degree).  0 launches the kernels one by one. */
-enum { LSMF_GMG_OPT_GRAPH = 1 };
+ * Chebyshev degree).  0 launches the kernels one by one.
+ * LSMF_GMG_OPT_SCATTER: LSMF_SCATTER_ATOMIC (default) or
+ * LSMF_SCATTER_COLOUR8 for every level operator, diagonal, restriction and
+ * prolongation (a bit-reproducible V-cycle). */
+enum { LSMF_GMG_OPT_GRAPH = 1, LSMF_GMG_OPT_SCATTER = 2 };
 lsmf_status lsmf_gmg_set_option(lsmf_gmg *g, int option, int value);
 
 /* ---- CG (SolverCG as driven by solve_linear_system, mf_elasticity.h:3012-3214) */
@@ -196,9 +225,6 @@ typedef struct {
 lsmf_status lsmf_cg_solve(lsmf_op *fine, int precond, double omega, lsmf_gmg *gmg, double *d_x,
                           const double *d_b, double tol_abs, int max_it, lsmf_solve_info *info);
 
-/* ---- residual (assemble_system rhs part, mf_elasticity.h:2708-2922) ---- */
-/* R = -int tau : grad^s N dV + f_ext, constrained entries zeroed; returns
- * ||R|| in *norm.  d_mu_cell / traction handled by the problem object. */
 
 /* ---- full problem: .prm driven load stepping (Solid::run) ---- */
 /* Parse a reference-format .prm text (ParameterHandler syntax, keys of
@@ -228,19 +254,36 @@ lsmf_status lsmf_problem_run(lsmf_problem *p, lsmf_newton_info *info);
 /* final displacement (host, n_dofs doubles) */
 lsmf_status lsmf_problem_get_solution(const lsmf_problem *p, double *host_u);
 
+/* ---- residual: the right-hand side part of assemble_system
+ * (mf_elasticity.h:2708-2922) for the problem's mesh, per-cell shear
+ * modulus, Poisson ratio and formulation:
+ *   R = -int tau(u) : grad N dV  (:2736-2804, FP64)
+ *       + int T(x, t) . N dA      (Neumann faces of the .prm, :2859-2892)
+ * with the entries of Dirichlet-constrained dofs set to zero (:2917-2921),
+ * and *norm = ||R||_2 over the dofs (the reference's error_residual).
+ * d_u, d_R: FP64 device vectors of n_dofs; t: load time of the traction
+ * expressions.  Waits for the problem's stream (norm is a host value). */
+lsmf_status lsmf_residual(lsmf_problem *p, const double *d_u, double t, double *d_R, double *norm);
+
 /* ---- allocation-free residual norm (no counterpart in the reference) ----
  * *d_norm = ||d_b - A d_x||_2 for a cached FP64 operator, computed without
- * any device allocation: for callers that cannot call cudaMalloc while they
- * run (their device memory is owned by another framework's caching
+ * calling cudaMalloc: for callers that cannot allocate device memory while
+ * they run (their device memory is owned by another framework's caching
  * allocator, or a no-allocation-after-start-up rule applies).  The scratch
  * (A x and the reduction partials) is a static device array of
- * LSMF_NOALLOC_MAX_DOFS + 1024 doubles (16 MiB) that every GPU loading the
- * library keeps until exit; operators with more dofs are rejected with
- * LSMF_ERR_INVALID_ARG.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress) and should come before any stream
- * capture.  All calls share the array, so calls that overlap on the GPU
- * (different streams, no ordering between them) race.  Asynchronous on the
- * operator's stream; d_norm is a device pointer to one double. */
+ * LSMF_NOALLOC_MAX_DOFS + 1024 doubles (16 MiB), kept by every GPU that has
+ * loaded it until exit; operators with more dofs are rejected with
+ * LSMF_ERR_INVALID_ARG.  Under CUDA's lazy module loading (the default) the
+ * array is placed in device memory when a device first uses it, that is at
+ * the first call on that device: make one call at start-up, before another
+ * framework's allocator reserves the pool, or set
+ * CUDA_MODULE_LOADING=EAGER.  That first call on a device should also come
+ * before any stream capture.  Every call looks up the array's device address
+ * (cudaGetSymbolAddress) for the operator's device, which must be current
+ * (else LSMF_ERR_INVALID_ARG).  All calls share the array, so calls that
+ * overlap on the GPU (different streams, no ordering between them) race.
+ * Asynchronous on the operator's stream; d_norm is a device pointer to one
+ * double. */
 #define LSMF_NOALLOC_MAX_DOFS 2097152
 lsmf_status lsmf_residual_norm_noalloc(lsmf_op *op, const double *d_x, const double *d_b, double *d_norm);
 

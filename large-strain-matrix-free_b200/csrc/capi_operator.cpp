@@ -124,6 +124,7 @@ lsmf_status lsmf_operator_create(lsmf_mesh *m, int level, lsmf_caching caching, 
   if (!op) return LSMF_ERR_ALLOC;
   op->mesh = m; op->level = level; op->caching = caching; op->formulation = formulation;
   op->precision = precision;
+  if (cudaGetDevice(&op->device) != cudaSuccess) { delete op; set_error("cudaGetDevice failed"); return LSMF_ERR_CUDA; }
   op->ncomp = table_components(caching, formulation, precision);
   const Level &L = op->L();
   lsmf_status s;
@@ -168,6 +169,19 @@ lsmf_status lsmf_operator_set_option(lsmf_op *op, int option, int value) {
     op->max_warps = value;
     return LSMF_OK;
   }
+  if (option == LSMF_OPT_WAIT_TRIES) {
+    if (value < -1) { set_error("wait tries must be -1 (default) or >= 0"); return LSMF_ERR_INVALID_ARG; }
+    op->wait_tries = value;
+    return LSMF_OK;
+  }
+  if (option == LSMF_OPT_SCATTER) {
+    if (value != LSMF_SCATTER_ATOMIC && value != LSMF_SCATTER_COLOUR8) {
+      set_error("scatter must be 0 (atomic) or 1 (colour8)");
+      return LSMF_ERR_INVALID_ARG;
+    }
+    op->scatter = value;
+    return LSMF_OK;
+  }
   set_error("unknown option");
   return LSMF_ERR_INVALID_ARG;
 }
@@ -207,6 +221,21 @@ lsmf_status lsmf_operator_vmult_add(lsmf_op *op, void *d_dst, const void *d_src)
   return launch_apply(op, d_dst, d_src, LSMF_MASK_DEFAULT, true);
 }
 
+lsmf_status lsmf_operator_sync(lsmf_op *op) {
+  if (!op) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  int flag = 0;
+  LSMF_CUDA(cudaMemcpyAsync(&flag, op->d_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, op->stream));
+  LSMF_CUDA(cudaStreamSynchronize(op->stream));
+  if (flag & 2) {
+    // reported once: the word is cleared for the calls that follow
+    LSMF_CUDA(cudaMemsetAsync(op->d_flag.ptr, 0, sizeof(int), op->stream));
+    LSMF_CUDA(cudaStreamSynchronize(op->stream));
+    set_error("a bounded device wait timed out in the vmult kernel; the result of that vmult is incomplete");
+    return LSMF_ERR_TIMEOUT;
+  }
+  return LSMF_OK;
+}
+
 lsmf_status lsmf_operator_compute_diagonal(lsmf_op *op) {
   if (!op) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
   if (!op->cached) { set_error("cache() has not been called"); return LSMF_ERR_NOT_INITIALIZED; }
@@ -230,6 +259,24 @@ lsmf_status lsmf_operator_precondition_jacobi(lsmf_op *op, void *d_dst, const vo
 }
 
 int lsmf_operator_m(const lsmf_op *op) { return op ? op->L().n_dofs() : 0; }
+
+int lsmf_operator_n(const lsmf_op *op) { return op ? op->L().n_dofs() : 0; }
+
+lsmf_status lsmf_operator_el(lsmf_op *op, int row, int col, double *value) {
+  if (!op || !value) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  if (row != col) { set_error("el() is only implemented on the diagonal (row == col)"); return LSMF_ERR_UNSUPPORTED; }
+  if (row < 0 || row >= op->L().n_dofs()) { set_error("row out of range"); return LSMF_ERR_INVALID_ARG; }
+  if (!op->have_diag) { set_error("compute_diagonal() has not been called"); return LSMF_ERR_NOT_INITIALIZED; }
+  LSMF_CUDA(cudaStreamSynchronize(op->stream));
+  if (op->precision == LSMF_FP64) {
+    LSMF_CUDA(cudaMemcpy(value, (const double *)op->d_diag.ptr + row, sizeof(double), cudaMemcpyDeviceToHost));
+  } else {
+    float f = 0;
+    LSMF_CUDA(cudaMemcpy(&f, (const float *)op->d_diag.ptr + row, sizeof(float), cudaMemcpyDeviceToHost));
+    *value = f;
+  }
+  return LSMF_OK;
+}
 
 size_t lsmf_operator_memory_consumption(const lsmf_op *op) {
   // cache tables + index maps (the reference excludes the diagonals too,

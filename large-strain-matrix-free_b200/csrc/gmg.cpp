@@ -359,9 +359,10 @@ lsmf_status vcycle(lsmf_gmg *g, int l) {
   LSMF_TRY(launch_apply(GL.op, GL.r.ptr, GL.x.ptr, LSMF_MASK_DEFAULT, false));
   LSMF_CUDA(cudaMemsetAsync(GC.b.ptr, 0, (size_t)GC.op->L().n_dofs() * sizeof(T), st));
   LSMF_TRY(restrict_add_async<T>(*M.levels[l - 1], *M.transfer[l], (const T *)GL.b.ptr, (const T *)GL.r.ptr,
-                                 (T *)GC.b.ptr, st));
+                                 (T *)GC.b.ptr, g->scatter, st));
   LSMF_TRY(vcycle<T>(g, l - 1));
-  LSMF_TRY(prolongate_add_async<T>(*M.levels[l - 1], *M.transfer[l], (const T *)GC.x.ptr, (T *)GL.x.ptr, st));
+  LSMF_TRY(prolongate_add_async<T>(*M.levels[l - 1], *M.transfer[l], (const T *)GC.x.ptr, (T *)GL.x.ptr, g->scatter,
+                                   st));
   LSMF_TRY(chebyshev_run<T>(g, l, (T *)GL.x.ptr, (const T *)GL.b.ptr, false));  // post-smoothing (step)
   return LSMF_OK;
 }
@@ -487,6 +488,17 @@ lsmf_status lsmf_gmg_set_option(lsmf_gmg *g, int option, int value) {
   if (!g) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
   if (option == LSMF_GMG_OPT_GRAPH) {
     g->use_graph = value != 0;
+    drop_graph(g);
+    return LSMF_OK;
+  }
+  if (option == LSMF_GMG_OPT_SCATTER) {
+    if (value != LSMF_SCATTER_ATOMIC && value != LSMF_SCATTER_COLOUR8) {
+      set_error("scatter must be 0 (atomic) or 1 (colour8)");
+      return LSMF_ERR_INVALID_ARG;
+    }
+    g->scatter = value;
+    for (auto &GL : g->levels) GL.op->scatter = value;
+    // the captured V-cycle holds the old launch sequence
     drop_graph(g);
     return LSMF_OK;
   }
@@ -627,7 +639,13 @@ lsmf_status lsmf_cg_solve(lsmf_op *A, int precond, double omega, lsmf_gmg *gmg, 
   LSMF_CUDA(cudaMemcpyAsync(&flag, A->d_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
   LSMF_CUDA(cudaStreamSynchronize(st));
   if (info) { info->iterations = it; info->residual = res; info->converged = conv ? 1 : 0; }
-  if (flag & 2) { set_error("a bounded device wait timed out in the vmult kernel"); return LSMF_ERR_TIMEOUT; }
+  if (flag & 2) {
+    // reported once: the word is cleared for the calls that follow
+    LSMF_CUDA(cudaMemsetAsync(A->d_flag.ptr, 0, sizeof(int), st));
+    LSMF_CUDA(cudaStreamSynchronize(st));
+    set_error("a bounded device wait timed out in the vmult kernel");
+    return LSMF_ERR_TIMEOUT;
+  }
   if (!conv) { set_error("CG did not reach the tolerance"); return LSMF_ERR_CG_NOT_CONVERGED; }
   return LSMF_OK;
 }

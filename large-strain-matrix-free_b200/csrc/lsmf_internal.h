@@ -93,6 +93,12 @@ struct Level {
   std::vector<int> bfaces;      // (cell, face, id)
   std::vector<uint8_t> cmask;   // per dof
   std::vector<int> constrained;
+  // cells grouped by lattice colour (i&1) + 2 (j&1) + 4 (k&1): cells of one
+  // colour share no node; colour c is colour_cells[colour_off[c] ..
+  // colour_off[c+1])
+  std::vector<int> colour_cells;
+  int colour_off[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  DevBuf<int> d_colour_cells;
   // device
   DevBuf<int> d_cell_nodes;     // packed with constraint bits
   DevBuf<double> d_X;
@@ -146,6 +152,9 @@ struct lsmf_op {
   int stages = -1;                   // bulk-copy (TMA) ring depth of the vmult kernel (0 = plain loads, -1 auto)
   bool basic = false;                // use the basic (smem-sweep) vmult kernel
   int max_warps = 0;                 // warps per block cap of the vmult kernel (<= 8, 0 auto)
+  int wait_tries = -1;               // bulk-copy wait bound (try_wait calls; -1 = default 2^22)
+  int device = 0;                    // CUDA device the operator's buffers live on
+  int scatter = LSMF_SCATTER_ATOMIC; // cell-loop scatter: atomics or the 8 colour launches
   cudaStream_t stream = 0;
   // CG workspace (outer FP64 CG driven through this operator)
   lsmf::DevBuf<double> cg_g, cg_h, cg_d, sc, partial;

@@ -298,6 +298,18 @@ lsmf_status build_mesh(lsmf_mesh &M) {
     if ((long long)L->n_nodes >= (1LL << NODE_BITS)) { set_error("too many nodes"); return LSMF_ERR_UNSUPPORTED; }
     LSMF_TRY(L->d_X.upload(L->X.data(), L->X.size()));
     LSMF_TRY(level_constraints(M, *L));
+    // cells by lattice colour: two cells of one colour are two or more
+    // lattice steps apart in some direction, so they share no node
+    L->colour_cells.clear();
+    for (int c = 0; c < 8; ++c) {
+      L->colour_off[c] = (int)L->colour_cells.size();
+      for (int e = 0; e < L->n_cells; ++e) {
+        const int *ijk = &L->cell_ijk[3 * (size_t)e];
+        if ((ijk[0] & 1) + 2 * (ijk[1] & 1) + 4 * (ijk[2] & 1) == c) L->colour_cells.push_back(e);
+      }
+    }
+    L->colour_off[8] = (int)L->colour_cells.size();
+    LSMF_TRY(L->d_colour_cells.upload(L->colour_cells.data(), L->colour_cells.size()));
   }
   M.transfer.assign(nl, nullptr);
   for (int l = 1; l < nl; ++l) {

@@ -9,11 +9,15 @@
 // residual of an operator they set up earlier.
 //
 // The scratch holds A x (at most LSMF_NOALLOC_MAX_DOFS doubles, 16 MiB) and
-// the per-block partial sums of the reduction.  Every GPU that loads the
-// library keeps this array until the process exits.
+// the per-block partial sums of the reduction.  Every GPU that loads this
+// file's module keeps the array until the process exits.  With CUDA's lazy
+// module loading (the default) the module, and with it the array, is placed
+// in device memory the first time a device uses it: at the first call of the
+// entry point on that device.  A caller whose memory pool is later taken by
+// another allocator makes one call at start-up (or sets
+// CUDA_MODULE_LOADING=EAGER), so that the 16 MiB are placed before the pool
+// is reserved.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "lsmf_internal.h"
 
@@ -25,15 +29,9 @@ namespace {
 
 constexpr size_t NOALLOC_PARTIALS = 1024;  // reduction blocks (fixed grid)
 constexpr int NOALLOC_THREADS = 256;
-constexpr int MAX_DEVICES = 64;
 
 // [0, LSMF_NOALLOC_MAX_DOFS): A x; then NOALLOC_PARTIALS partial sums
 static __device__ __align__(256) double g_scratch[LSMF_NOALLOC_MAX_DOFS + NOALLOC_PARTIALS];
-
-// device address of g_scratch, looked up once per device (host code must not
-// use the symbol itself: on the host it only names a stand-in)
-double *g_scratch_addr[MAX_DEVICES] = {nullptr};
-std::mutex g_setup_mutex;
 
 __global__ void residual_partials_kernel(const double *__restrict__ ax, const double *__restrict__ b, size_t n,
                                          double *partial) {
@@ -67,22 +65,22 @@ __global__ void sqrt_sum_kernel(const double *partial, int n, double *out) {
   }
 }
 
-// Device address of the scratch array on the current device; the first call
-// on a device resolves it with that device current.
-lsmf_status scratch_address(double **out) {
+// Device address of the scratch array for the operator's device.  Host code
+// must not pass g_scratch itself to a kernel: on the host that name is only a
+// stand-in, not a device address.  The address is looked up on every call (a
+// host-side table lookup once the module is loaded), so it stays right after
+// the device's context was reset and the module placed again.
+lsmf_status scratch_address(const lsmf_op *op, double **out) {
   int dev = 0;
   LSMF_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= MAX_DEVICES) {
-    lsmf::set_error("device index out of range for the allocation-free entry point");
-    return LSMF_ERR_UNSUPPORTED;
+  if (dev != op->device) {
+    lsmf::set_error("the operator lives on device " + std::to_string(op->device) + " but device " +
+                    std::to_string(dev) + " is current; make the operator's device current first");
+    return LSMF_ERR_INVALID_ARG;
   }
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[dev]) {
-    void *p = nullptr;
-    LSMF_CUDA(cudaGetSymbolAddress(&p, g_scratch));
-    g_scratch_addr[dev] = (double *)p;
-  }
-  *out = g_scratch_addr[dev];
+  void *p = nullptr;
+  LSMF_CUDA(cudaGetSymbolAddress(&p, g_scratch));
+  *out = (double *)p;
   return LSMF_OK;
 }
 
@@ -101,7 +99,7 @@ extern "C" lsmf_status lsmf_residual_norm_noalloc(lsmf_op *op, const double *d_x
     return LSMF_ERR_INVALID_ARG;
   }
   double *scratch = nullptr;
-  LSMF_TRY(scratch_address(&scratch));
+  LSMF_TRY(scratch_address(op, &scratch));
   double *ax = scratch, *partial = scratch + LSMF_NOALLOC_MAX_DOFS;
   // A x into the scratch (the vmult overwrites every entry it owns: zero, cell
   // contributions, identity rows), then the fused (b - A x)^2 reduction

@@ -272,6 +272,7 @@ lsmf_status parse_prm(const std::string &text, ProblemParams &P) {
       else if (key == "MF level precision") P.level_precision = val;             // additive
       else if (key == "MF Chebyshev degree") ok = to_int(val, P.cheb_degree);     // additive
       else if (key == "MF Chebyshev smoothing range") ok = to_double(val, P.smoothing_range);  // additive
+      else if (key == "MF scatter") P.scatter = val;                             // additive
       else known = false;
     } else if (sec == "Nonlinear solver") {
       if (key == "Max iterations Newton-Raphson") ok = to_int(val, P.max_nr);

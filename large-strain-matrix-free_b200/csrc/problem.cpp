@@ -255,6 +255,19 @@ struct Timer {
   }
 };
 
+// R = fext - f_int(u) with the constrained entries zeroed: the right-hand
+// side of assemble_system (mf_elasticity.h:2736-2921); fext is the device
+// Neumann load of the step
+lsmf_status residual_async(lsmf_problem *pb, const double *u, const double *fext, double *R) {
+  const Level &L = *pb->mesh->levels.back();
+  const size_t n = (size_t)L.n_dofs();
+  cudaStream_t st = pb->stream;
+  LSMF_CUDA(cudaMemcpyAsync(R, fext, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  LSMF_TRY(internal_force_async(L, pb->mesh->basis, u, pb->mu_dev.ptr, pb->prm.nu, pb->prm.formulation, R,
+                                pb->op->scatter, st));
+  return set_indexed_async<double>(R, L.d_constrained.ptr, (int)L.constrained.size(), 0.0, st);
+}
+
 // "gmg-gc" (global coarsening, mf_elasticity.h:1597-1632, 1892-1916) builds
 // its levels by coarsening the triangulation; on the structured meshes here,
 // which are refined globally and have no hanging nodes, that sequence is the
@@ -300,9 +313,7 @@ lsmf_status problem_run(lsmf_problem *pb, lsmf_newton_info *info) {
       Timer tr(st);
       LSMF_CUDA(cudaMemcpyAsync(u_tot, u_n, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
       LSMF_TRY(axpy_async<double>(u_tot, 1.0, du, n, st));
-      LSMF_CUDA(cudaMemcpyAsync(R, pb->fext.ptr, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
-      LSMF_TRY(internal_force_async(L, pb->mesh->basis, u_tot, pb->mu_dev.ptr, P.nu, P.formulation, R, st));
-      LSMF_TRY(set_indexed_async<double>(R, cidx, nc, 0.0, st));
+      LSMF_TRY(residual_async(pb, u_tot, pb->fext.ptr, R));
       bool cached = false;
       if (it == 0 && inhom) {
         // rhs -= K g over the constrained columns (the inhomogeneity that
@@ -417,6 +428,10 @@ static lsmf_status validate_params(const ProblemParams &P, int &caching) {
     set_error("MF level precision must be float or double");
     return LSMF_ERR_PRM;
   }
+  if (P.scatter != "atomic" && P.scatter != "colour8") {
+    set_error("MF scatter must be atomic or colour8");
+    return LSMF_ERR_PRM;
+  }
   if (P.type != "Cook" && P.type != "Box") {
     set_error("Geometry Type " + P.type + " is not supported (Cook | Box)");
     return LSMF_ERR_UNSUPPORTED;
@@ -490,6 +505,13 @@ lsmf_status lsmf_problem_create(const char *text, lsmf_problem **out) {
     gd.coarse_chebyshev = P.coarse_chebyshev;
     gd.coarse_accurate_eig = P.coarse_accurate_eig;
     if ((s = lsmf_gmg_create(pb->mesh, &gd, &pb->gmg)) != LSMF_OK) { delete pb; return s; }
+  }
+  if (P.scatter == "colour8") {
+    pb->op->scatter = LSMF_SCATTER_COLOUR8;
+    if (pb->gmg && (s = lsmf_gmg_set_option(pb->gmg, LSMF_GMG_OPT_SCATTER, LSMF_SCATTER_COLOUR8)) != LSMF_OK) {
+      delete pb;
+      return s;
+    }
   }
   const Level &L = *pb->mesh->levels.back();
   const size_t n = (size_t)L.n_dofs();
@@ -569,6 +591,19 @@ lsmf_status lsmf_problem_set_stream(lsmf_problem *pb, void *stream) {
 lsmf_status lsmf_problem_run(lsmf_problem *pb, lsmf_newton_info *info) {
   if (!pb) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
   return problem_run(pb, info);
+}
+
+lsmf_status lsmf_residual(lsmf_problem *pb, const double *d_u, double t, double *d_R, double *norm) {
+  if (!pb || !d_u || !d_R) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  const size_t n = (size_t)pb->mesh->levels.back()->n_dofs();
+  std::vector<double> fext;
+  neumann_load(*pb, t, fext);
+  LSMF_TRY(pb->fext.upload(fext.data(), n));
+  LSMF_TRY(residual_async(pb, d_u, pb->fext.ptr, d_R));
+  const double r = norm_of(pb, d_R);
+  if (!(r == r)) { set_error("residual norm is not a number"); return LSMF_ERR_CUDA; }
+  if (norm) *norm = r;
+  return LSMF_OK;
 }
 
 lsmf_status lsmf_problem_get_solution(const lsmf_problem *pb, double *host_u) {

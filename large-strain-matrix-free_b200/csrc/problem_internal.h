@@ -33,7 +33,7 @@ struct BCExpr {
 // additive keys without a reference counterpart: Geometry / Type = Box, Box
 // cells, Box lower / upper corner, Void spheres, Cook thickness; Linear
 // solver / MF level precision, MF Chebyshev degree, MF Chebyshev smoothing
-// range.
+// range, MF scatter.
 struct ProblemParams {
   // Finite element system
   int degree = 2, quad_order = 3;
@@ -51,6 +51,7 @@ struct ProblemParams {
   int formulation = 0;
   // Linear solver
   std::string solver_type = "CG", precond = "jacobi", caching = "scalar", level_precision = "float";
+  std::string scatter = "atomic";  // atomic | colour8 (bit-reproducible cell loops)
   double tol_lin = 1e-6, relaxation = 0.65, amg_threshold = 1e-4, smoothing_range = 20.0;
   int max_it_mult = 1, cond_cg_its = 20, cheb_eig_its = 30, cheb_degree = 5;
   bool coarse_chebyshev = true, coarse_accurate_eig = true;

@@ -60,15 +60,19 @@ lsmf_status cheb_first_async(T *x, T *xold, const T *b, T *r, const T *invd, con
 template <typename T>
 lsmf_status cheb_step_async(T *x, T *xold, const T *b, T *r, const T *invd, const uint8_t *cmask, double f1, double f2,
                             bool has_old, size_t n, cudaStream_t st);
+// scatter: LSMF_SCATTER_ATOMIC, or LSMF_SCATTER_COLOUR8 (one launch per
+// colour of the coarse cells, plain adds, bit-reproducible)
 template <typename T>
-lsmf_status restrict_add_async(const Level &C, const TransferMap &TM, const T *b, const T *r, T *coarse, cudaStream_t st);
+lsmf_status restrict_add_async(const Level &C, const TransferMap &TM, const T *b, const T *r, T *coarse, int scatter,
+                               cudaStream_t st);
 template <typename T>
-lsmf_status prolongate_add_async(const Level &C, const TransferMap &TM, const T *coarse, T *fine, cudaStream_t st);
+lsmf_status prolongate_add_async(const Level &C, const TransferMap &TM, const T *coarse, T *fine, int scatter,
+                                 cudaStream_t st);
 template <typename T>
 lsmf_status interpolate_async(const Level &C, const Level &F, const TransferMap &TM, const T *fine_u, T *coarse_u,
                               cudaStream_t st);
 lsmf_status internal_force_async(const Level &L, const Basis &B, const double *u, const double *mu, double nu,
-                                 int formulation, double *R, cudaStream_t st);
+                                 int formulation, double *R, int scatter, cudaStream_t st);
 lsmf_status adjoint_cell_grad_async(const Level &L, const Basis &B, const double *u, const double *mu, double nu,
                                     int formulation, const double *lam, double *grad, cudaStream_t st);
 // apply with an un-zeroed gather of constrained entries (K g over the
@@ -116,6 +120,7 @@ struct lsmf_gmg {
   // set-up (vstale) and applied to the executable graph in place when the
   // launch sequence is unchanged
   bool use_graph = true;
+  int scatter = LSMF_SCATTER_ATOMIC;  // cell loops and transfers: atomics or colour8
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t vexec = nullptr;
   bool vstale = true;

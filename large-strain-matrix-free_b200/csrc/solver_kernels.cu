@@ -417,16 +417,20 @@ struct Prol1D {
 
 // one warp per coarse cell.  restriction: coarse += R (weight * (b - r))
 // on the fine level, coarse Dirichlet entries dropped (restrict_and_add).
+// cells / plain: the coarse cells of one lattice colour (no two share a
+// node) with plain adds, or (cells == nullptr) all n_coarse cells with
+// atomics.
 template <int P, typename T>
-__global__ void restrict_kernel(int n_coarse, const int *__restrict__ coarse_cn, const int *__restrict__ fine_nodes,
-                                const double *__restrict__ weight, const T *__restrict__ b, const T *__restrict__ r,
-                                T *coarse, Prol1D<P> pm) {
+__global__ void restrict_kernel(int n_coarse, const int *__restrict__ cells, int plain, const int *__restrict__ coarse_cn,
+                                const int *__restrict__ fine_nodes, const double *__restrict__ weight,
+                                const T *__restrict__ b, const T *__restrict__ r, T *coarse, Prol1D<P> pm) {
   constexpr int N1 = P + 1, NF = 2 * P + 1, NFB = NF * NF * NF, NCN = N1 * N1 * N1;
   constexpr int SZ = 3 * NFB + 3 * NF * NF * N1 + 3 * NF * N1 * N1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
   double *in = (double *)smem_raw + warp * SZ, *s1 = in + 3 * NFB, *s2 = s1 + 3 * NF * NF * N1;
-  for (int c = blockIdx.x * wpb + warp; c < n_coarse; c += gridDim.x * wpb) {
+  for (int ic = blockIdx.x * wpb + warp; ic < n_coarse; ic += gridDim.x * wpb) {
+    const int c = cells ? __ldg(cells + ic) : ic;
     const int *fn = fine_nodes + (size_t)c * NFB;
     // gather the fine block: all node ids of the lane first, then all
     // weights and values, so every load of the lane is in flight at once
@@ -478,7 +482,11 @@ __global__ void restrict_kernel(int n_coarse, const int *__restrict__ coarse_cn,
 #pragma unroll
       for (int fx = 0; fx < NF; ++fx) s += pm.m[fx][x] * s2[zy * NF + fx + k * N1 * N1 * NF];
       const int packed = coarse_cn[(size_t)c * NCN + a];
-      if (!((packed >> (NODE_BITS + k)) & 1)) atomicAdd(coarse + 3 * (size_t)(packed & NODE_MASK) + k, T(s));
+      if (!((packed >> (NODE_BITS + k)) & 1)) {
+        T *dst = coarse + 3 * (size_t)(packed & NODE_MASK) + k;
+        if (plain) *dst += T(s);
+        else atomicAdd(dst, T(s));
+      }
     }
     __syncwarp();
   }
@@ -486,7 +494,8 @@ __global__ void restrict_kernel(int n_coarse, const int *__restrict__ coarse_cn,
 
 // prolongation: fine += P coarse (coarse Dirichlet entries read as zero)
 template <int P, typename T>
-__global__ void prolongate_kernel(int n_coarse, const int *__restrict__ coarse_cn, const int *__restrict__ fine_nodes,
+__global__ void prolongate_kernel(int n_coarse, const int *__restrict__ cells, int plain,
+                                  const int *__restrict__ coarse_cn, const int *__restrict__ fine_nodes,
                                   const double *__restrict__ weight, const T *__restrict__ coarse, T *fine, Prol1D<P> pm) {
   constexpr int N1 = P + 1, NF = 2 * P + 1, NFB = NF * NF * NF, NCN = N1 * N1 * N1;
   constexpr int SZ = 3 * NCN + 3 * N1 * N1 * NF + 3 * N1 * NF * NF;
@@ -494,7 +503,8 @@ __global__ void prolongate_kernel(int n_coarse, const int *__restrict__ coarse_c
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
   double *v = (double *)smem_raw + warp * SZ, *s1 = v + 3 * NCN, *s2 = s1 + 3 * N1 * N1 * NF;
   constexpr int NPL = (NFB + 31) / 32;
-  for (int c = blockIdx.x * wpb + warp; c < n_coarse; c += gridDim.x * wpb) {
+  for (int ic = blockIdx.x * wpb + warp; ic < n_coarse; ic += gridDim.x * wpb) {
+    const int c = cells ? __ldg(cells + ic) : ic;
     // the lane's fine nodes and weights, loaded before the sweeps
     const int *fn = fine_nodes + (size_t)c * NFB;
     int node[NPL];
@@ -536,7 +546,9 @@ __global__ void prolongate_kernel(int n_coarse, const int *__restrict__ coarse_c
         double s = 0;
 #pragma unroll
         for (int z = 0; z < N1; ++z) s += pm.m[fz][z] * s2[(k * N1 + z) * NF * NF + fyx];
-        atomicAdd(fine + 3 * (size_t)node[q] + k, T(w[q] * s));
+        T *dst = fine + 3 * (size_t)node[q] + k;
+        if (plain) *dst += T(w[q] * s);
+        else atomicAdd(dst, T(w[q] * s));
       }
     }
     __syncwarp();
@@ -566,6 +578,7 @@ __global__ void interpolate_kernel(int n_coarse_nodes, int ncn, const int *__res
 // MODE 0: scatter into R; MODE 1: grad[cell] = lambda . (cell vector)
 template <int P, int Q, int MODE>
 __global__ void __launch_bounds__(128) internal_force_kernel(const int *__restrict__ cell_nodes, int n_cells,
+                                                              const int *__restrict__ cells, int plain,
                                                               const double *__restrict__ X, const double *__restrict__ u,
                                                               const double *__restrict__ mu_cell, double nu, int formulation,
                                                               double *R, const double *__restrict__ lam, double *grad,
@@ -575,7 +588,8 @@ __global__ void __launch_bounds__(128) internal_force_kernel(const int *__restri
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
   double *slab = (double *)smem_raw + warp * S::SZ;
-  for (int cell = blockIdx.x * wpb + warp; cell < n_cells; cell += gridDim.x * wpb) {
+  for (int ic = blockIdx.x * wpb + warp; ic < n_cells; ic += gridDim.x * wpb) {
+    const int cell = cells ? __ldg(cells + ic) : ic;
     const int *cn = cell_nodes + (size_t)cell * NN;
     int ck[RPL][N1];
     double vx[RPL][N1], vu[RPL][N1];
@@ -670,7 +684,10 @@ __global__ void __launch_bounds__(128) internal_force_kernel(const int *__restri
 #pragma unroll
       for (int i = 0; i < N1; ++i) {
         const size_t dof = 3 * (size_t)(ck[r][i] & NODE_MASK) + comp;
-        if (MODE == 0) atomicAdd(R + dof, out[r][i]);
+        if (MODE == 0) {
+          if (plain) R[dof] += out[r][i];
+          else atomicAdd(R + dof, out[r][i]);
+        }
         else acc += lam[dof] * out[r][i];
       }
     }
@@ -898,9 +915,23 @@ static Prol1D<P> make_prol(const TransferMap &T) {
   return pm;
 }
 
+// Run f(cells, n, plain) over all cells of L (atomics), or with the colour8
+// scatter once per lattice colour in the order 0..7 (plain adds).
+template <typename F>
+static lsmf_status over_colours(const Level &L, int scatter, F &&f) {
+  if (scatter == LSMF_SCATTER_COLOUR8) {
+    for (int c = 0; c < 8; ++c) {
+      const int n = L.colour_off[c + 1] - L.colour_off[c];
+      if (n > 0) LSMF_TRY(f(L.d_colour_cells.ptr + L.colour_off[c], n, 1));
+    }
+    return LSMF_OK;
+  }
+  return f((const int *)nullptr, L.n_cells, 0);
+}
+
 template <typename T, int P>
 static lsmf_status transfer_impl(bool restrict_dir, const Level &C, const TransferMap &TM, const T *b, const T *r,
-                                 T *coarse_or_fine, const T *coarse_src, cudaStream_t st) {
+                                 T *coarse_or_fine, const T *coarse_src, int scatter, cudaStream_t st) {
   constexpr int N1 = P + 1, NF = 2 * P + 1;
   const int wpb = 4;
   const Prol1D<P> pm = make_prol<P>(TM);
@@ -909,50 +940,59 @@ static lsmf_status transfer_impl(bool restrict_dir, const Level &C, const Transf
     const size_t smem = sizeof(double) * SZ * wpb;
     auto k = restrict_kernel<P, T>;
     LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int g = (C.n_cells + wpb - 1) / wpb;
-    if (g > 16 * sms()) g = 16 * sms();
-    k<<<g, 32 * wpb, smem, st>>>(C.n_cells, C.d_cell_nodes.ptr, TM.d_fine_nodes.ptr, TM.d_weight.ptr, b, r,
-                                  coarse_or_fine, pm);
+    LSMF_TRY(over_colours(C, scatter, [&](const int *cells, int n, int plain) -> lsmf_status {
+      int g = (n + wpb - 1) / wpb;
+      if (g > 16 * sms()) g = 16 * sms();
+      k<<<g, 32 * wpb, smem, st>>>(n, cells, plain, C.d_cell_nodes.ptr, TM.d_fine_nodes.ptr, TM.d_weight.ptr, b, r,
+                                    coarse_or_fine, pm);
+      return LSMF_OK;
+    }));
   } else {
     constexpr int SZ = 3 * N1 * N1 * N1 + 3 * N1 * N1 * NF + 3 * N1 * NF * NF;
     const size_t smem = sizeof(double) * SZ * wpb;
     auto k = prolongate_kernel<P, T>;
     LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int g = (C.n_cells + wpb - 1) / wpb;
-    if (g > 16 * sms()) g = 16 * sms();
-    k<<<g, 32 * wpb, smem, st>>>(C.n_cells, C.d_cell_nodes.ptr, TM.d_fine_nodes.ptr, TM.d_weight.ptr, coarse_src,
-                                  coarse_or_fine, pm);
+    LSMF_TRY(over_colours(C, scatter, [&](const int *cells, int n, int plain) -> lsmf_status {
+      int g = (n + wpb - 1) / wpb;
+      if (g > 16 * sms()) g = 16 * sms();
+      k<<<g, 32 * wpb, smem, st>>>(n, cells, plain, C.d_cell_nodes.ptr, TM.d_fine_nodes.ptr, TM.d_weight.ptr,
+                                    coarse_src, coarse_or_fine, pm);
+      return LSMF_OK;
+    }));
   }
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
 }
 
 template <typename T>
-lsmf_status restrict_add_async(const Level &C, const TransferMap &TM, const T *b, const T *r, T *coarse, cudaStream_t st) {
+lsmf_status restrict_add_async(const Level &C, const TransferMap &TM, const T *b, const T *r, T *coarse, int scatter,
+                               cudaStream_t st) {
   switch (C.p) {
-    case 1: return transfer_impl<T, 1>(true, C, TM, b, r, coarse, nullptr, st);
-    case 2: return transfer_impl<T, 2>(true, C, TM, b, r, coarse, nullptr, st);
-    case 3: return transfer_impl<T, 3>(true, C, TM, b, r, coarse, nullptr, st);
-    case 4: return transfer_impl<T, 4>(true, C, TM, b, r, coarse, nullptr, st);
+    case 1: return transfer_impl<T, 1>(true, C, TM, b, r, coarse, nullptr, scatter, st);
+    case 2: return transfer_impl<T, 2>(true, C, TM, b, r, coarse, nullptr, scatter, st);
+    case 3: return transfer_impl<T, 3>(true, C, TM, b, r, coarse, nullptr, scatter, st);
+    case 4: return transfer_impl<T, 4>(true, C, TM, b, r, coarse, nullptr, scatter, st);
   }
   return LSMF_ERR_UNSUPPORTED;
 }
 template <typename T>
-lsmf_status prolongate_add_async(const Level &C, const TransferMap &TM, const T *coarse, T *fine, cudaStream_t st) {
+lsmf_status prolongate_add_async(const Level &C, const TransferMap &TM, const T *coarse, T *fine, int scatter,
+                                 cudaStream_t st) {
   switch (C.p) {
-    case 1: return transfer_impl<T, 1>(false, C, TM, nullptr, nullptr, fine, coarse, st);
-    case 2: return transfer_impl<T, 2>(false, C, TM, nullptr, nullptr, fine, coarse, st);
-    case 3: return transfer_impl<T, 3>(false, C, TM, nullptr, nullptr, fine, coarse, st);
-    case 4: return transfer_impl<T, 4>(false, C, TM, nullptr, nullptr, fine, coarse, st);
+    case 1: return transfer_impl<T, 1>(false, C, TM, nullptr, nullptr, fine, coarse, scatter, st);
+    case 2: return transfer_impl<T, 2>(false, C, TM, nullptr, nullptr, fine, coarse, scatter, st);
+    case 3: return transfer_impl<T, 3>(false, C, TM, nullptr, nullptr, fine, coarse, scatter, st);
+    case 4: return transfer_impl<T, 4>(false, C, TM, nullptr, nullptr, fine, coarse, scatter, st);
   }
   return LSMF_ERR_UNSUPPORTED;
 }
 template lsmf_status restrict_add_async<float>(const Level &, const TransferMap &, const float *, const float *, float *,
-                                               cudaStream_t);
+                                               int, cudaStream_t);
 template lsmf_status restrict_add_async<double>(const Level &, const TransferMap &, const double *, const double *,
-                                                double *, cudaStream_t);
-template lsmf_status prolongate_add_async<float>(const Level &, const TransferMap &, const float *, float *, cudaStream_t);
-template lsmf_status prolongate_add_async<double>(const Level &, const TransferMap &, const double *, double *,
+                                                double *, int, cudaStream_t);
+template lsmf_status prolongate_add_async<float>(const Level &, const TransferMap &, const float *, float *, int,
+                                                 cudaStream_t);
+template lsmf_status prolongate_add_async<double>(const Level &, const TransferMap &, const double *, double *, int,
                                                   cudaStream_t);
 
 template <typename T>
@@ -970,7 +1010,8 @@ template lsmf_status interpolate_async<double>(const Level &, const Level &, con
 
 template <int P, int Q, int MODE>
 static lsmf_status internal_force_impl(const Level &L, const Basis &B, const double *u, const double *mu, double nu,
-                                       int formulation, double *R, const double *lam, double *grad, cudaStream_t st) {
+                                       int formulation, double *R, const double *lam, double *grad, int scatter,
+                                       cudaStream_t st) {
   using S = SFR<P, Q, double>;
   TabT<P, Q, double> t;
   Tab<P, Q> w;
@@ -987,21 +1028,27 @@ static lsmf_status internal_force_impl(const Level &L, const Basis &B, const dou
   const size_t smem = sizeof(double) * S::SZ * wpb;
   auto k = internal_force_kernel<P, Q, MODE>;
   LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int g = (L.n_cells + wpb - 1) / wpb;
-  if (g > 16 * sms()) g = 16 * sms();
-  k<<<g, 32 * wpb, smem, st>>>(L.d_cell_nodes.ptr, L.n_cells, L.d_X.ptr, u, mu, nu, formulation, R, lam, grad, t, w);
+  // the cell gradient (MODE 1) writes one value per cell and needs no colours
+  LSMF_TRY(over_colours(L, MODE == 0 ? scatter : LSMF_SCATTER_ATOMIC,
+                        [&](const int *cells, int n, int plain) -> lsmf_status {
+                          int g = (n + wpb - 1) / wpb;
+                          if (g > 16 * sms()) g = 16 * sms();
+                          k<<<g, 32 * wpb, smem, st>>>(L.d_cell_nodes.ptr, n, cells, plain, L.d_X.ptr, u, mu, nu,
+                                                        formulation, R, lam, grad, t, w);
+                          return LSMF_OK;
+                        }));
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;
 }
 
 // R += -f_int(u) (caller initialises R with the external load)
 lsmf_status internal_force_async(const Level &L, const Basis &B, const double *u, const double *mu, double nu,
-                                 int formulation, double *R, cudaStream_t st) {
+                                 int formulation, double *R, int scatter, cudaStream_t st) {
   switch (L.p) {
-    case 1: return internal_force_impl<1, 2, 0>(L, B, u, mu, nu, formulation, R, nullptr, nullptr, st);
-    case 2: return internal_force_impl<2, 3, 0>(L, B, u, mu, nu, formulation, R, nullptr, nullptr, st);
-    case 3: return internal_force_impl<3, 4, 0>(L, B, u, mu, nu, formulation, R, nullptr, nullptr, st);
-    case 4: return internal_force_impl<4, 5, 0>(L, B, u, mu, nu, formulation, R, nullptr, nullptr, st);
+    case 1: return internal_force_impl<1, 2, 0>(L, B, u, mu, nu, formulation, R, nullptr, nullptr, scatter, st);
+    case 2: return internal_force_impl<2, 3, 0>(L, B, u, mu, nu, formulation, R, nullptr, nullptr, scatter, st);
+    case 3: return internal_force_impl<3, 4, 0>(L, B, u, mu, nu, formulation, R, nullptr, nullptr, scatter, st);
+    case 4: return internal_force_impl<4, 5, 0>(L, B, u, mu, nu, formulation, R, nullptr, nullptr, scatter, st);
   }
   return LSMF_ERR_UNSUPPORTED;
 }
@@ -1009,10 +1056,10 @@ lsmf_status internal_force_async(const Level &L, const Basis &B, const double *u
 lsmf_status adjoint_cell_grad_async(const Level &L, const Basis &B, const double *u, const double *mu, double nu,
                                     int formulation, const double *lam, double *grad, cudaStream_t st) {
   switch (L.p) {
-    case 1: return internal_force_impl<1, 2, 1>(L, B, u, mu, nu, formulation, nullptr, lam, grad, st);
-    case 2: return internal_force_impl<2, 3, 1>(L, B, u, mu, nu, formulation, nullptr, lam, grad, st);
-    case 3: return internal_force_impl<3, 4, 1>(L, B, u, mu, nu, formulation, nullptr, lam, grad, st);
-    case 4: return internal_force_impl<4, 5, 1>(L, B, u, mu, nu, formulation, nullptr, lam, grad, st);
+    case 1: return internal_force_impl<1, 2, 1>(L, B, u, mu, nu, formulation, nullptr, lam, grad, LSMF_SCATTER_ATOMIC, st);
+    case 2: return internal_force_impl<2, 3, 1>(L, B, u, mu, nu, formulation, nullptr, lam, grad, LSMF_SCATTER_ATOMIC, st);
+    case 3: return internal_force_impl<3, 4, 1>(L, B, u, mu, nu, formulation, nullptr, lam, grad, LSMF_SCATTER_ATOMIC, st);
+    case 4: return internal_force_impl<4, 5, 1>(L, B, u, mu, nu, formulation, nullptr, lam, grad, LSMF_SCATTER_ATOMIC, st);
   }
   return LSMF_ERR_UNSUPPORTED;
 }

@@ -20,6 +20,7 @@ LIB_PATH = os.path.join(HERE, "liblsmf.so")
 
 CACHING = {"scalar": 0, "tensor2": 1, "tensor4": 2, "scalar_referential": 3, "tensor4_ns": 4}
 GEOM = {"box": 0, "cook": 1}
+SCATTER = {"atomic": 0, "colour8": 1}
 MASK_ZERO, MASK_MPI, MASK_RW, MASK_SF, MASK_QD, MASK_DEFAULT = 1, 2, 4, 8, 16, 31
 
 
@@ -80,9 +81,12 @@ SIGNATURES = {
     "lsmf_operator_get_diagonal": (ctypes.c_int, [vp, ctypes.POINTER(vp), ctypes.POINTER(vp)]),
     "lsmf_operator_precondition_jacobi": (ctypes.c_int, [vp, vp, vp, ctypes.c_double]),
     "lsmf_operator_m": (ctypes.c_int, [vp]),
+    "lsmf_operator_n": (ctypes.c_int, [vp]),
+    "lsmf_operator_el": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, dp]),
     "lsmf_operator_memory_consumption": (ctypes.c_size_t, [vp]),
     "lsmf_operator_set_stream": (ctypes.c_int, [vp, vp]),
     "lsmf_operator_set_option": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+    "lsmf_operator_sync": (ctypes.c_int, [vp]),
     "lsmf_operator_get_table": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.POINTER(ctypes.c_size_t)]),
     "lsmf_gmg_create": (ctypes.c_int, [vp, ctypes.POINTER(GmgDesc), ctypes.POINTER(vp)]),
     "lsmf_gmg_destroy": (None, [vp]),
@@ -102,6 +106,7 @@ SIGNATURES = {
     "lsmf_problem_run": (ctypes.c_int, [vp, ctypes.POINTER(NewtonInfo)]),
     "lsmf_problem_set_stream": (ctypes.c_int, [vp, vp]),
     "lsmf_problem_get_solution": (ctypes.c_int, [vp, dp]),
+    "lsmf_residual": (ctypes.c_int, [vp, vp, ctypes.c_double, vp, dp]),
     "lsmf_adjoint_forward": (ctypes.c_int, [vp, dp, dp, ctypes.c_int, dp]),
     "lsmf_adjoint_backward": (ctypes.c_int, [vp, dp]),
     "lsmf_residual_norm_noalloc": (ctypes.c_int, [vp, vp, vp, vp]),
@@ -225,7 +230,8 @@ class NeoHookOperator:
     def m(self):
         return lib().lsmf_operator_m(self.h)
 
-    n = m
+    def n(self):
+        return lib().lsmf_operator_n(self.h)
 
     def set_material(self, mu_per_cell, nu):
         nc, _, _ = self.mesh.info(self.level)
@@ -262,9 +268,9 @@ class NeoHookOperator:
         return self._diag_tensors()[0]
 
     def el(self, row, col):
-        if row != col:
-            raise LsmfError(10, "el() is only defined on the diagonal")
-        return float(self.get_matrix_diagonal()[row])
+        v = ctypes.c_double()
+        check(lib().lsmf_operator_el(self.h, int(row), int(col), ctypes.byref(v)))
+        return v.value
 
     def precondition_Jacobi(self, dst, src, omega):
         check(lib().lsmf_operator_precondition_jacobi(self.h, _dptr(dst), _dptr(src), omega))
@@ -284,6 +290,21 @@ class NeoHookOperator:
 
     def set_max_warps(self, w):
         check(lib().lsmf_operator_set_option(self.h, 3, int(w)))
+
+    def set_wait_tries(self, tries):
+        """Bound of the pipelined kernel's wait for a cell record (-1 =
+        default; 0 makes every wait run out at once, for tests)."""
+        check(lib().lsmf_operator_set_option(self.h, 4, int(tries)))
+
+    def set_scatter(self, mode):
+        """'atomic' (default) or 'colour8' (8 colour launches, plain adds:
+        bit-reproducible)."""
+        check(lib().lsmf_operator_set_option(self.h, 5, SCATTER[mode] if isinstance(mode, str) else int(mode)))
+
+    def sync(self):
+        """Wait for the operator's stream; raises LsmfError (status 8) if a
+        bounded device wait ran out since the last call."""
+        check(lib().lsmf_operator_sync(self.h))
 
     def set_stream(self, stream):
         """Order every call on a CUDA stream (torch.cuda.Stream or raw handle)."""
@@ -343,6 +364,10 @@ class GMG:
         """Replay the V-cycle as one CUDA graph (default) or launch kernel by kernel."""
         check(lib().lsmf_gmg_set_option(self.h, 1, int(bool(enable))))
 
+    def set_scatter(self, mode):
+        """'atomic' (default) or 'colour8' for every level cell loop and transfer."""
+        check(lib().lsmf_gmg_set_option(self.h, 2, SCATTER[mode] if isinstance(mode, str) else int(mode)))
+
     def level_info(self, level):
         out = np.zeros(6)
         check(lib().lsmf_gmg_level_info(self.h, level, out.ctypes.data_as(dp)))
@@ -400,6 +425,13 @@ class Problem:
                   "point_u": [info.point_u[i][c] for c in range(3)]} for i in range(info.n_steps)]
         return {"status": st, "steps": steps, "time_residual": info.time_residual,
                 "time_setup": info.time_setup, "time_solve": info.time_solve}
+
+    def residual(self, u, t, R):
+        """assemble_system's right-hand side R = f_ext(t) - f_int(u), Dirichlet
+        entries zeroed, into the device vector R; returns ||R||."""
+        nrm = ctypes.c_double()
+        check(lib().lsmf_residual(self.h, _dptr(u), float(t), _dptr(R), ctypes.byref(nrm)))
+        return nrm.value
 
     def solution(self):
         u = np.zeros(self.n_dofs)

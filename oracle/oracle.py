@@ -311,17 +311,58 @@ class NewtonParams(ctypes.Structure):
                  ("neu_ab", ctypes.c_double * 48)])
 
 
+def _splitmix64(state):
+    state = (state + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+    z = state
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+    return state, z ^ (z >> 31)
+
+
+def void_mask(cells, count, radius, seed, lo=(0, 0, 0), hi=(1, 1, 1)):
+    """Coarse-cell mask of the heterogeneous-voids geometry (the benchmark's
+    "unit cube with seeded non-overlapping spherical voids"): sphere centres
+    drawn uniformly (splitmix64 stream of the seed) inside the box shrunk by
+    the radius, a candidate kept when it is at least 2.5 radii from every
+    kept centre, until `count` are kept; a coarse cell is removed (0) when
+    its centre lies inside a sphere.  Returns uint8[cz][cy][cx] flattened,
+    x fastest."""
+    state = (seed * 0x2545F4914F6CDD1D + 1) & 0xFFFFFFFFFFFFFFFF
+    centres, tries = [], 0
+    while len(centres) < count and tries < 100000:
+        tries += 1
+        pt = []
+        for d in range(3):
+            state, z = _splitmix64(state)
+            u01 = (z >> 11) * (1.0 / 9007199254740992.0)
+            pt.append(lo[d] + radius + u01 * ((hi[d] - lo[d]) - 2 * radius))
+        if all(np.sqrt(sum((pt[d] - c[d]) ** 2 for d in range(3))) >= 2.0 * radius * 1.25 for c in centres):
+            centres.append(pt)
+    nx, ny, nz = cells
+    act = np.ones(nx * ny * nz, dtype=np.uint8)
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                x = (lo[0] + (i + 0.5) * (hi[0] - lo[0]) / nx, lo[1] + (j + 0.5) * (hi[1] - lo[1]) / ny,
+                     lo[2] + (k + 0.5) * (hi[2] - lo[2]) / nz)
+                for c in centres:
+                    if sum((x[d] - c[d]) ** 2 for d in range(3)) < radius * radius:
+                        act[(k * ny + j) * nx + i] = 0
+    return act
+
+
 def newton(geometry=GEOM_BOX, coarse=(1, 1, 1), n_refinements=0, lo=(0, 0, 0), hi=(1, 1, 1), scale=1.0,
            p=2, q=3, caching="tensor4", formulation=1, mu=1.0, nu=0.3, mu_fine=None,
            dirichlet=(), neumann=(), end_time=1.0, dt=0.1, max_nr=10, tol_f=1e-9, tol_u=1e-6,
            tol_f_abs=0.0, tol_u_abs=0.0, tol_lin=1e-6, max_it_mult=1, precond="gmg", relaxation=0.65,
            cheb_degree=5, cheb_eig_its=30, smoothing_range=20.0, coarse_chebyshev=True,
-           coarse_accurate_eig=True, level_fp32=True, output_point=None, return_u=False):
+           coarse_accurate_eig=True, level_fp32=True, output_point=None, return_u=False, coarse_active=None):
     """Run the oracle's load-stepping Newton solve.
 
     dirichlet: list of (id, comp_mask_bits, (v0, v1, v2)) — values are the
     increment imposed at the first Newton iteration of each step.
     neumann: list of (id, a[3], b[3]) with traction a + b * t.
+    coarse_active: optional coarse-cell mask (uint8, x fastest), e.g. void_mask().
     """
     P = NewtonParams()
     for k in range(3):
@@ -355,11 +396,13 @@ def newton(geometry=GEOM_BOX, coarse=(1, 1, 1), n_refinements=0, lo=(0, 0, 0), h
     cg = np.zeros(100000, dtype=np.int32)
     mu_arr = None if mu_fine is None else np.ascontiguousarray(mu_fine, dtype=np.float64)
     # size the displacement output from a mesh of the same description
-    m = Mesh(geometry, coarse, n_refinements, lo, hi, scale, p, q)
+    act = None if coarse_active is None else np.ascontiguousarray(coarse_active, dtype=np.uint8)
+    m = Mesh(geometry, coarse, n_refinements, lo, hi, scale, p, q, coarse_active=act)
     u = np.zeros(m.n_dofs)
     rc = lib().orc_newton(ctypes.byref(P), _p(mu_arr) if mu_arr is not None else None,
                           ctypes.byref(n_cells), ctypes.byref(n_dofs), ctypes.byref(vol), max_steps,
-                          _p(steps), ctypes.byref(nsteps), _p(u), _p(cg), len(cg))
+                          _p(steps), ctypes.byref(nsteps), _p(u), _p(cg), len(cg),
+                          _p(act) if act is not None else None)
     out = {"rc": rc, "n_cells": n_cells.value, "n_dofs": n_dofs.value, "volume": vol.value,
            "steps": [{"time": s[0], "newton_iterations": int(s[1]), "converged": bool(s[2]),
                       "point_u": s[3:6].copy(), "cg_iterations": int(s[6])}

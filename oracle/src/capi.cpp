@@ -257,12 +257,16 @@ struct orc_newton_params {
 };
 
 // out_steps: per step [time, newton_its, converged, u0, u1, u2, total_cg_its]
+// coarse_active (optional, coarse[0]*coarse[1]*coarse[2] bytes, x fastest):
+// coarse cells removed from the mesh (the voids geometry)
 int orc_newton(const orc_newton_params *P, const double *mu_fine, int *n_cells, int *n_dofs,
                double *volume, int max_steps, double *out_steps, int *n_steps, double *u_out,
-               int *cg_its_out, int max_cg_entries) {
+               int *cg_its_out, int max_cg_entries, const uint8_t *coarse_active) {
   try {
     NewtonParams prm;
     prm.mesh.geometry = P->geometry;
+    if (coarse_active)
+      prm.mesh.coarse_active.assign(coarse_active, coarse_active + (size_t)P->coarse[0] * P->coarse[1] * P->coarse[2]);
     for (int k = 0; k < 3; ++k) { prm.mesh.coarse[k] = P->coarse[k]; prm.mesh.lo[k] = P->lo[k]; prm.mesh.hi[k] = P->hi[k]; }
     prm.mesh.n_refinements = P->n_refinements; prm.mesh.scale = P->scale;
     prm.mesh.p = P->p; prm.mesh.q = P->q;

@@ -11,7 +11,7 @@ SECTIONS = {
                       "Preconditioner relaxation", "Preconditioner AMG aggregation threshold",
                       "Condition number CG iterations", "MF caching", "MF Chebyshev number CG iterations",
                       "MF Chebyshev coarse", "MF Chebyshev coarse accurate eigenvalues", "MF level precision",
-                      "MF Chebyshev degree", "MF Chebyshev smoothing range"],
+                      "MF Chebyshev degree", "MF Chebyshev smoothing range", "MF scatter"],
     "Nonlinear solver": ["Max iterations Newton-Raphson", "Tolerance force", "Absolute tolerance force",
                          "Tolerance displacement", "Absolute tolerance displacement"],
     "Time": ["End time", "Time step size"],
