@@ -255,7 +255,7 @@ class GMG:
 
     def __init__(self, geometry, coarse, n_refinements, lo, hi, scale, p, q, caching, formulation, fp32, mu_fine, nu,
                  dirichlet, u, degree=5, smoothing_range=20.0, eig_its=30, coarse_chebyshev=True,
-                 coarse_accurate_eig=True):
+                 coarse_accurate_eig=True, coarse_active=None):
         L = lib()
         L.orc_gmg_new.restype = ctypes.c_void_p
         L.orc_gmg_vmult.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
@@ -267,12 +267,14 @@ class GMG:
         ids = np.array([d[0] for d in dirichlet] or [0], dtype=np.int32)
         masks = np.array([d[1] for d in dirichlet] or [0], dtype=np.int32)
         uu = np.ascontiguousarray(u, dtype=np.float64)
+        self._act = None if coarse_active is None else np.ascontiguousarray(coarse_active, dtype=np.uint8)
         self.h = L.orc_gmg_new(ctypes.c_int(geometry), _ip(c), ctypes.c_int(n_refinements), _dp(lo_), _dp(hi_),
                                ctypes.c_double(scale), ctypes.c_int(p), ctypes.c_int(q), ctypes.c_int(CACHE[caching]),
                                ctypes.c_int(formulation), ctypes.c_int(int(fp32)), _dp(mu), ctypes.c_double(nu),
                                ctypes.c_int(len(dirichlet)), _ip(ids), _ip(masks), _dp(uu), ctypes.c_int(degree),
                                ctypes.c_double(smoothing_range), ctypes.c_int(eig_its),
-                               ctypes.c_int(int(coarse_chebyshev)), ctypes.c_int(int(coarse_accurate_eig)))
+                               ctypes.c_int(int(coarse_chebyshev)), ctypes.c_int(int(coarse_accurate_eig)),
+                               _p(self._act) if self._act is not None else None)
         if not self.h:
             raise RuntimeError(L.orc_last_error().decode())
         self.n = uu.size
@@ -351,19 +353,13 @@ def void_mask(cells, count, radius, seed, lo=(0, 0, 0), hi=(1, 1, 1)):
     return act
 
 
-def newton(geometry=GEOM_BOX, coarse=(1, 1, 1), n_refinements=0, lo=(0, 0, 0), hi=(1, 1, 1), scale=1.0,
+def _params(geometry=GEOM_BOX, coarse=(1, 1, 1), n_refinements=0, lo=(0, 0, 0), hi=(1, 1, 1), scale=1.0,
            p=2, q=3, caching="tensor4", formulation=1, mu=1.0, nu=0.3, mu_fine=None,
            dirichlet=(), neumann=(), end_time=1.0, dt=0.1, max_nr=10, tol_f=1e-9, tol_u=1e-6,
            tol_f_abs=0.0, tol_u_abs=0.0, tol_lin=1e-6, max_it_mult=1, precond="gmg", relaxation=0.65,
            cheb_degree=5, cheb_eig_its=30, smoothing_range=20.0, coarse_chebyshev=True,
-           coarse_accurate_eig=True, level_fp32=True, output_point=None, return_u=False, coarse_active=None):
-    """Run the oracle's load-stepping Newton solve.
-
-    dirichlet: list of (id, comp_mask_bits, (v0, v1, v2)) — values are the
-    increment imposed at the first Newton iteration of each step.
-    neumann: list of (id, a[3], b[3]) with traction a + b * t.
-    coarse_active: optional coarse-cell mask (uint8, x fastest), e.g. void_mask().
-    """
+           coarse_accurate_eig=True, level_fp32=True, output_point=None):
+    """The flat parameter block of orc_newton / orc_adjoint."""
     P = NewtonParams()
     for k in range(3):
         P.lo[k], P.hi[k], P.coarse[k] = lo[k], hi[k], coarse[k]
@@ -389,11 +385,32 @@ def newton(geometry=GEOM_BOX, coarse=(1, 1, 1), n_refinements=0, lo=(0, 0, 0), h
         P.neu_ids[i] = bid
         for c in range(3):
             P.neu_ab[6 * i + c], P.neu_ab[6 * i + 3 + c] = a[c], b[c]
+    return P
+
+
+def newton(geometry=GEOM_BOX, coarse=(1, 1, 1), n_refinements=0, lo=(0, 0, 0), hi=(1, 1, 1), scale=1.0,
+           p=2, q=3, caching="tensor4", formulation=1, mu=1.0, nu=0.3, mu_fine=None,
+           dirichlet=(), neumann=(), end_time=1.0, dt=0.1, max_nr=10, tol_f=1e-9, tol_u=1e-6,
+           tol_f_abs=0.0, tol_u_abs=0.0, tol_lin=1e-6, max_it_mult=1, precond="gmg", relaxation=0.65,
+           cheb_degree=5, cheb_eig_its=30, smoothing_range=20.0, coarse_chebyshev=True,
+           coarse_accurate_eig=True, level_fp32=True, output_point=None, return_u=False, coarse_active=None):
+    """Run the oracle's load-stepping Newton solve.
+
+    dirichlet: list of (id, comp_mask_bits, (v0, v1, v2)) — values are the
+    increment imposed at the first Newton iteration of each step.
+    neumann: list of (id, a[3], b[3]) with traction a + b * t.
+    coarse_active: optional coarse-cell mask (uint8, x fastest), e.g. void_mask().
+    """
+    P = _params(geometry, coarse, n_refinements, lo, hi, scale, p, q, caching, formulation, mu, nu, mu_fine,
+                dirichlet, neumann, end_time, dt, max_nr, tol_f, tol_u, tol_f_abs, tol_u_abs, tol_lin, max_it_mult,
+                precond, relaxation, cheb_degree, cheb_eig_its, smoothing_range, coarse_chebyshev,
+                coarse_accurate_eig, level_fp32, output_point)
     n_cells, n_dofs, nsteps = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
     vol = ctypes.c_double()
     max_steps = 1000
     steps = np.zeros((max_steps, 7))
     cg = np.zeros(100000, dtype=np.int32)
+    hist = np.full((20000, 3), -1.0)
     mu_arr = None if mu_fine is None else np.ascontiguousarray(mu_fine, dtype=np.float64)
     # size the displacement output from a mesh of the same description
     act = None if coarse_active is None else np.ascontiguousarray(coarse_active, dtype=np.uint8)
@@ -402,11 +419,39 @@ def newton(geometry=GEOM_BOX, coarse=(1, 1, 1), n_refinements=0, lo=(0, 0, 0), h
     rc = lib().orc_newton(ctypes.byref(P), _p(mu_arr) if mu_arr is not None else None,
                           ctypes.byref(n_cells), ctypes.byref(n_dofs), ctypes.byref(vol), max_steps,
                           _p(steps), ctypes.byref(nsteps), _p(u), _p(cg), len(cg),
-                          _p(act) if act is not None else None)
+                          _p(act) if act is not None else None, _p(hist), len(hist))
     out = {"rc": rc, "n_cells": n_cells.value, "n_dofs": n_dofs.value, "volume": vol.value,
            "steps": [{"time": s[0], "newton_iterations": int(s[1]), "converged": bool(s[2]),
                       "point_u": s[3:6].copy(), "cg_iterations": int(s[6])}
                      for s in steps[:nsteps.value]]}
+    hist = hist[hist[:, 0] >= 0]
+    for i, s in enumerate(out["steps"]):
+        h = hist[hist[:, 0] == i]
+        s["rel_res"], s["rel_upd"] = h[:, 1].copy(), h[:, 2].copy()
     if return_u:
         out["u"] = u
     return out
+
+
+def adjoint(log_mu, u_target, obj_id, coarse_active=None, **kw):
+    """The oracle's FP64 adjoint gradient: forward Newton solve with mu =
+    exp(log_mu) per fine cell (keyword arguments as for newton()), then
+    K(u) lambda = dJ/du by CG with the FP64 V-cycle to 1e-13, then
+    dJ/dlog mu_c = lambda . dR/dlog mu_c with tau differentiated in mu.
+    Returns (J, grad per cell, u)."""
+    keys = _params.__code__.co_varnames[:_params.__code__.co_argcount]
+    P = _params(**{k: v for k, v in kw.items() if k in keys})
+    act = None if coarse_active is None else np.ascontiguousarray(coarse_active, dtype=np.uint8)
+    m = Mesh(P.geometry, tuple(P.coarse), P.n_refinements, tuple(P.lo), tuple(P.hi), P.scale, P.p, P.q,
+             coarse_active=act)
+    lm = np.ascontiguousarray(log_mu, dtype=np.float64)
+    tg = np.ascontiguousarray(u_target, dtype=np.float64)
+    assert lm.size == m.n_cells and tg.size == m.n_dofs
+    J = ctypes.c_double()
+    g = np.zeros(m.n_cells)
+    u = np.zeros(m.n_dofs)
+    rc = lib().orc_adjoint(ctypes.byref(P), _p(act) if act is not None else None, _p(lm), _p(tg),
+                           ctypes.c_int(obj_id), ctypes.byref(J), _p(g), _p(u))
+    if rc != 0:
+        raise RuntimeError("oracle adjoint failed (%d): %s" % (rc, lib().orc_last_error().decode()))
+    return J.value, g, u

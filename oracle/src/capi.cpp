@@ -199,12 +199,14 @@ struct GmgH {
 void *orc_gmg_new(int geom, const int *coarse, int nref, const double *lo, const double *hi, double scale, int p,
                   int q, int caching, int formulation, int fp32, const double *mu_fine, double nu, int n_dir,
                   const int *dir_ids, const int *dir_masks, const double *u, int degree, double range, int eig_its,
-                  int coarse_cheb, int coarse_accurate) {
+                  int coarse_cheb, int coarse_accurate, const uint8_t *coarse_active) {
   try {
     auto *h = new GmgH();
     NewtonParams &P = h->prm;
     P.mesh.geometry = geom; P.mesh.n_refinements = nref; P.mesh.scale = scale; P.mesh.p = p; P.mesh.q = q;
     for (int k = 0; k < 3; ++k) { P.mesh.coarse[k] = coarse[k]; P.mesh.lo[k] = lo[k]; P.mesh.hi[k] = hi[k]; }
+    if (coarse_active)
+      P.mesh.coarse_active.assign(coarse_active, coarse_active + (size_t)coarse[0] * coarse[1] * coarse[2]);
     P.caching = caching; P.formulation = formulation; P.nu = nu;
     P.cheb_degree = degree; P.smoothing_range = range; P.cheb_eig_its = eig_its;
     P.coarse_chebyshev = coarse_cheb; P.coarse_accurate_eig = coarse_accurate;
@@ -256,39 +258,45 @@ struct orc_newton_params {
   double neu_ab[48];
 };
 
+static NewtonParams to_params(const orc_newton_params *P, const uint8_t *coarse_active) {
+  NewtonParams prm;
+  prm.mesh.geometry = P->geometry;
+  if (coarse_active)
+    prm.mesh.coarse_active.assign(coarse_active, coarse_active + (size_t)P->coarse[0] * P->coarse[1] * P->coarse[2]);
+  for (int k = 0; k < 3; ++k) { prm.mesh.coarse[k] = P->coarse[k]; prm.mesh.lo[k] = P->lo[k]; prm.mesh.hi[k] = P->hi[k]; }
+  prm.mesh.n_refinements = P->n_refinements; prm.mesh.scale = P->scale;
+  prm.mesh.p = P->p; prm.mesh.q = P->q;
+  prm.caching = P->caching; prm.formulation = P->formulation;
+  prm.mu = P->mu; prm.nu = P->nu;
+  prm.end_time = P->end_time; prm.dt = P->dt; prm.max_nr = P->max_nr;
+  prm.tol_f = P->tol_f; prm.tol_u = P->tol_u; prm.tol_f_abs = P->tol_f_abs; prm.tol_u_abs = P->tol_u_abs;
+  prm.tol_lin = P->tol_lin; prm.max_it_mult = P->max_it_mult; prm.precond = P->precond;
+  prm.relaxation = P->relaxation; prm.cheb_degree = P->cheb_degree; prm.cheb_eig_its = P->cheb_eig_its;
+  prm.smoothing_range = P->smoothing_range;
+  prm.coarse_chebyshev = P->coarse_chebyshev; prm.coarse_accurate_eig = P->coarse_accurate_eig;
+  prm.level_fp32 = P->level_fp32; prm.has_output_point = P->has_output_point;
+  for (int k = 0; k < 3; ++k) prm.output_point[k] = P->output_point[k];
+  for (int i = 0; i < P->n_dirichlet; ++i) {
+    prm.dirichlet.push_back({P->dir_ids[i], P->dir_masks[i]});
+    prm.dirichlet_value.push_back({P->dir_values[3 * i], P->dir_values[3 * i + 1], P->dir_values[3 * i + 2]});
+  }
+  for (int i = 0; i < P->n_neumann; ++i) {
+    Neumann nm; nm.id = P->neu_ids[i];
+    for (int c = 0; c < 3; ++c) { nm.a[c] = P->neu_ab[6 * i + c]; nm.b[c] = P->neu_ab[6 * i + 3 + c]; }
+    prm.neumann.push_back(nm);
+  }
+  return prm;
+}
+
 // out_steps: per step [time, newton_its, converged, u0, u1, u2, total_cg_its]
 // coarse_active (optional, coarse[0]*coarse[1]*coarse[2] bytes, x fastest):
 // coarse cells removed from the mesh (the voids geometry)
 int orc_newton(const orc_newton_params *P, const double *mu_fine, int *n_cells, int *n_dofs,
                double *volume, int max_steps, double *out_steps, int *n_steps, double *u_out,
-               int *cg_its_out, int max_cg_entries, const uint8_t *coarse_active) {
+               int *cg_its_out, int max_cg_entries, const uint8_t *coarse_active, double *hist_out,
+               int max_hist_entries) {
   try {
-    NewtonParams prm;
-    prm.mesh.geometry = P->geometry;
-    if (coarse_active)
-      prm.mesh.coarse_active.assign(coarse_active, coarse_active + (size_t)P->coarse[0] * P->coarse[1] * P->coarse[2]);
-    for (int k = 0; k < 3; ++k) { prm.mesh.coarse[k] = P->coarse[k]; prm.mesh.lo[k] = P->lo[k]; prm.mesh.hi[k] = P->hi[k]; }
-    prm.mesh.n_refinements = P->n_refinements; prm.mesh.scale = P->scale;
-    prm.mesh.p = P->p; prm.mesh.q = P->q;
-    prm.caching = P->caching; prm.formulation = P->formulation;
-    prm.mu = P->mu; prm.nu = P->nu;
-    prm.end_time = P->end_time; prm.dt = P->dt; prm.max_nr = P->max_nr;
-    prm.tol_f = P->tol_f; prm.tol_u = P->tol_u; prm.tol_f_abs = P->tol_f_abs; prm.tol_u_abs = P->tol_u_abs;
-    prm.tol_lin = P->tol_lin; prm.max_it_mult = P->max_it_mult; prm.precond = P->precond;
-    prm.relaxation = P->relaxation; prm.cheb_degree = P->cheb_degree; prm.cheb_eig_its = P->cheb_eig_its;
-    prm.smoothing_range = P->smoothing_range;
-    prm.coarse_chebyshev = P->coarse_chebyshev; prm.coarse_accurate_eig = P->coarse_accurate_eig;
-    prm.level_fp32 = P->level_fp32; prm.has_output_point = P->has_output_point;
-    for (int k = 0; k < 3; ++k) prm.output_point[k] = P->output_point[k];
-    for (int i = 0; i < P->n_dirichlet; ++i) {
-      prm.dirichlet.push_back({P->dir_ids[i], P->dir_masks[i]});
-      prm.dirichlet_value.push_back({P->dir_values[3 * i], P->dir_values[3 * i + 1], P->dir_values[3 * i + 2]});
-    }
-    for (int i = 0; i < P->n_neumann; ++i) {
-      Neumann nm; nm.id = P->neu_ids[i];
-      for (int c = 0; c < 3; ++c) { nm.a[c] = P->neu_ab[6 * i + c]; nm.b[c] = P->neu_ab[6 * i + 3 + c]; }
-      prm.neumann.push_back(nm);
-    }
+    NewtonParams prm = to_params(P, coarse_active);
     NewtonResult res;
     if (mu_fine) {
       Mesh tmp; build_mesh(prm.mesh, prm.mesh.n_refinements, tmp);
@@ -297,7 +305,7 @@ int orc_newton(const orc_newton_params *P, const double *mu_fine, int *n_cells, 
     int rc = newton_run(prm, res);
     *n_cells = res.n_cells; *n_dofs = res.n_dofs; *volume = res.volume;
     *n_steps = (int)res.steps.size();
-    int cgk = 0;
+    int cgk = 0, hk = 0;
     for (int s = 0; s < (int)res.steps.size() && s < max_steps; ++s) {
       const auto &st = res.steps[s];
       double *o = out_steps + 7 * s;
@@ -305,10 +313,32 @@ int orc_newton(const orc_newton_params *P, const double *mu_fine, int *n_cells, 
       o[3] = st.point_u[0]; o[4] = st.point_u[1]; o[5] = st.point_u[2];
       int tot = 0;
       for (int c : st.cg_iterations) { tot += c; if (cg_its_out && cgk < max_cg_entries) cg_its_out[cgk++] = c; }
+      // hist_out: per load step and Newton iteration (step, rel_res, rel_upd)
+      for (size_t k = 0; k < st.rel_res.size(); ++k)
+        if (hist_out && hk < max_hist_entries) {
+          hist_out[3 * hk] = s; hist_out[3 * hk + 1] = st.rel_res[k]; hist_out[3 * hk + 2] = st.rel_upd[k];
+          ++hk;
+        }
       o[6] = tot;
     }
     if (u_out && !res.u.empty()) std::memcpy(u_out, res.u.data(), sizeof(double) * res.u.size());
     return rc;
+  } catch (std::exception &e) { g_err = e.what(); return -1; }
+}
+
+// Adjoint gradient (see adjoint_run): log_mu per fine cell, u_target per dof;
+// outputs J, grad (per fine cell) and the converged displacement.
+int orc_adjoint(const orc_newton_params *P, const uint8_t *coarse_active, const double *log_mu, const double *u_target,
+                int obj_id, double *J, double *grad, double *u_out) {
+  try {
+    NewtonParams prm = to_params(P, coarse_active);
+    Mesh m; build_mesh(prm.mesh, prm.mesh.n_refinements, m);
+    std::vector<double> lm(log_mu, log_mu + m.n_cells), tg(u_target, u_target + m.n_dofs()), g, u;
+    const int rc = adjoint_run(prm, lm, tg, obj_id, *J, g, u);
+    if (rc) return rc;
+    std::memcpy(grad, g.data(), sizeof(double) * g.size());
+    if (u_out) std::memcpy(u_out, u.data(), sizeof(double) * u.size());
+    return 0;
   } catch (std::exception &e) { g_err = e.what(); return -1; }
 }
 

@@ -158,6 +158,12 @@ double residual(const Mesh &m, const Basis1D &b, const std::vector<double> &mu,
                 const std::vector<Neumann> &neu, double time,
                 const std::vector<uint8_t> &cmask, double *R);
 
+// Adjoint building block: g[c] = lambda . dR/dlog mu_c for every cell, with
+// R the internal-force part of the residual (mf_elasticity.h:2736-2804) and
+// tau differentiated in mu (lambda(mu), kappa(mu) of material.h:82-94).
+void dresidual_dlogmu_dot(const Mesh &m, const Basis1D &b, const std::vector<double> &mu, double nu,
+                          int formulation, const double *u, const double *lam, double *g);
+
 // ------------------------------------------------ single-cell element matrix
 // Independent FEValues-style assembly in the reference configuration
 // (tests/mf_neo_hook_operator.cc:300-470 and mf_elasticity.h:2760-2843):

@@ -195,6 +195,92 @@ static double residual_impl(const Mesh &m, const Basis1D &bas, const std::vector
   return std::sqrt(nrm);
 }
 
+// d tau / d mu at a fixed deformation: get_tau (material.h:119-163)
+// differentiated in the shear modulus, with lambda = 2 mu nu / (1 - 2 nu) and
+// kappa = 2 mu (1 + nu) / (3 (1 - 2 nu)) (material.h:82-94) moving with it.
+//   formulation 1: tau = mu b - (mu - 2 lambda ln J) I
+//                  dtau/dmu = b - (1 - 2 lambda' ln J) I,  lambda' = 2 nu / (1 - 2 nu)
+//   formulation 0: tau = (J dPsi_vol/dJ - tr(tau_bar) / 3) I + tau_bar,
+//                  tau_bar = 2 c_1 b_bar = mu b_bar, dPsi_vol/dJ = kappa/2 (J - 1/J)
+//                  dtau/dmu = (J kappa'/2 (J - 1/J) - tr(b_bar) / 3) I + b_bar
+static void dtau_dmu(const Material &mat, double det_F, const double bbar[3][3], const double b[3][3],
+                     double out[3][3]) {
+  const double nu = mat.nu;
+  if (mat.formulation == 0) {
+    const double dkappa = 2.0 * (1.0 + nu) / (3.0 * (1.0 - 2.0 * nu));
+    const double vol = det_F * (dkappa / 2.0) * (det_F - 1.0 / det_F);
+    const double tr = bbar[0][0] + bbar[1][1] + bbar[2][2];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) out[i][j] = bbar[i][j] + (i == j ? vol - tr / 3.0 : 0.0);
+  } else {
+    const double dlambda = 2.0 * nu / (1.0 - 2.0 * nu);
+    const double d = 1.0 - 2.0 * dlambda * std::log(det_F);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) out[i][j] = b[i][j] - (i == j ? d : 0.0);
+  }
+}
+
+// g[c] = mu_c * lambda . dR_c/dmu_c for every cell c, where R_c is the cell's
+// internal-force part of the residual (mf_elasticity.h:2736-2804),
+// dR_c/dmu = -int dtau/dmu : grad_x N dV: the derivative of the residual with
+// respect to log mu_c, contracted with the adjoint vector.
+template <int P, int Q>
+static void dresidual_dlogmu_impl(const Mesh &m, const Basis1D &bas, const std::vector<double> &mu, double nu,
+                                  int formulation, const double *u, const double *lam, double *g) {
+  using CO = CellOps<P, Q, double>;
+  constexpr int NN = CO::NN, NQ = CO::NQ;
+  typename CO::Tables t; CO::tables(bas, t);
+#pragma omp parallel for schedule(static)
+  for (int cell = 0; cell < m.n_cells; ++cell) {
+    const int *nodes = &m.cell_nodes[(size_t)cell * NN];
+    double xl[3 * NN], ul[3 * NN];
+    for (int a = 0; a < NN; ++a)
+      for (int c = 0; c < 3; ++c) {
+        xl[c * NN + a] = m.X[3 * (size_t)nodes[a] + c];
+        ul[c * NN + a] = u[3 * (size_t)nodes[a] + c];
+      }
+    double GX[3][3][NQ], GU[3][3][NQ], H[3][3][NQ];
+    CO::grad(t, xl, GX);
+    CO::grad(t, ul, GU);
+    const Material mat(mu[cell], nu, formulation);
+    for (int q = 0; q < NQ; ++q) {
+      double Jr[3][3], Jri[3][3], gu[3][3];
+      for (int d = 0; d < 3; ++d)
+        for (int e = 0; e < 3; ++e) Jr[d][e] = GX[d][e][q];
+      const double jxw = inv3(Jr, Jri) * t.w[q];
+      for (int c = 0; c < 3; ++c)
+        for (int d = 0; d < 3; ++d) {
+          double a = 0;
+          for (int e = 0; e < 3; ++e) a += GU[c][e][q] * Jri[e][d];
+          gu[c][d] = a;
+        }
+      Kin k; kinematics(gu, k);
+      double dt[3][3]; dtau_dmu(mat, k.det, k.bbar, k.b, dt);
+      for (int c = 0; c < 3; ++c)
+        for (int f = 0; f < 3; ++f) {
+          double a = 0;
+          for (int d = 0; d < 3; ++d) {
+            double jf = 0;
+            for (int e = 0; e < 3; ++e) jf += Jri[f][e] * k.Fi[e][d];
+            a += dt[c][d] * jf;
+          }
+          H[c][f][q] = -a * jxw;
+        }
+    }
+    double out[3 * NN];
+    CO::integrate(t, H, out);
+    double s = 0;
+    for (int a = 0; a < NN; ++a)
+      for (int c = 0; c < 3; ++c) s += lam[3 * (size_t)nodes[a] + c] * out[c * NN + a];
+    g[cell] = mu[cell] * s;
+  }
+}
+
+void dresidual_dlogmu_dot(const Mesh &m, const Basis1D &b, const std::vector<double> &mu, double nu,
+                          int formulation, const double *u, const double *lam, double *g) {
+  DISPATCH_PQ(m.p, b.q, { dresidual_dlogmu_impl<P_, Q_>(m, b, mu, nu, formulation, u, lam, g); });
+}
+
 double residual(const Mesh &m, const Basis1D &b, const std::vector<double> &mu, double nu,
                 int formulation, const double *u, const std::vector<Neumann> &neu,
                 double time, const std::vector<uint8_t> &cmask, double *R) {

@@ -566,6 +566,8 @@ int newton_run(const NewtonParams &prm, NewtonResult &res) {
       }
       if (it == 0) err_res0 = err_res;
       const double rel_res = err_res0 != 0 ? err_res / err_res0 : err_res;
+      sr.rel_res.push_back(rel_res);
+      sr.rel_upd.push_back(err_upd_norm);
       if (it > 2) {
         if (err_res <= prm.tol_f_abs || err_upd <= prm.tol_u_abs) conv = true;
         if (rel_res <= prm.tol_f && err_upd_norm <= prm.tol_u) conv = true;
@@ -614,6 +616,63 @@ int newton_run(const NewtonParams &prm, NewtonResult &res) {
     time += prm.dt;
   }
   res.u = u_n;
+  return 0;
+}
+
+// Gradient of J(u(theta)) = 1/2 sum over the dofs on boundary `obj_id` of
+// (u - u_target)^2 with respect to theta_c = log mu_c (no reference
+// counterpart: the check of the device adjoint).  Forward: the load-stepping
+// Newton solve with mu = exp(theta).  Adjoint: K(u) lambda = dJ/du (the
+// symmetric tangent at the converged u, Dirichlet rows identity with zero
+// right-hand side) by CG with the FP64 V-cycle to 1e-13 of ||dJ/du||.
+// Gradient: dJ/dtheta_c = lambda . dR/dtheta_c, since R(u, theta) = 0 gives
+// du/dtheta = K^-1 dR/dtheta.
+int adjoint_run(const NewtonParams &prm_in, const std::vector<double> &log_mu, const std::vector<double> &target,
+                int obj_id, double &J, std::vector<double> &grad, std::vector<double> &u) {
+  NewtonParams prm = prm_in;
+  Basis1D bas; bas.init(prm.mesh.p, prm.mesh.q);
+  const int nl = prm.mesh.n_refinements + 1;
+  std::vector<Mesh> meshes(nl);
+  for (int l = 0; l < nl; ++l) build_mesh(prm.mesh, l, meshes[l]);
+  const Mesh &m = meshes[nl - 1];
+  if ((int)log_mu.size() != m.n_cells || (int)target.size() != m.n_dofs()) return 5;
+  prm.mu_fine.resize(m.n_cells);
+  for (int c = 0; c < m.n_cells; ++c) prm.mu_fine[c] = std::exp(log_mu[c]);
+  NewtonResult res;
+  const int rc = newton_run(prm, res);
+  if (rc) return rc;
+  u = res.u;
+  std::vector<std::vector<double>> lmu(nl);
+  for (int l = 0; l < nl; ++l) lmu[l] = coarsen_cell_field(meshes, l, prm.mu_fine);
+  std::vector<std::vector<uint8_t>> lmask(nl);
+  for (int l = 0; l < nl; ++l) constrained_dofs(meshes[l], prm.dirichlet, lmask[l]);
+  const std::vector<uint8_t> &cmask = lmask[nl - 1];
+  std::vector<uint8_t> obj;
+  constrained_dofs(m, {DirichletSpec{obj_id, 7}}, obj);
+  const size_t n = m.n_dofs();
+  std::vector<double> rhs(n, 0.0), lam(n, 0.0);
+  J = 0;
+  for (size_t i = 0; i < n; ++i)
+    if (obj[i]) {
+      const double r = u[i] - target[i];
+      J += 0.5 * r * r;
+      if (!cmask[i]) rhs[i] = r;
+    }
+  Operator<double> op;
+  op.initialize(&m, &bas, prm.caching, prm.formulation);
+  op.set_material(lmu[nl - 1], prm.nu);
+  op.set_constraints(cmask);
+  if (op.cache(u.data())) return 2;
+  GMG<double> gmg;
+  setup_gmg<double>(prm, meshes, bas, lmask, lmu, u, gmg, true);
+  auto Am = [&](std::vector<double> &d, const std::vector<double> &s) { op.vmult(d.data(), s.data()); };
+  auto Pm = [&](std::vector<double> &d, const std::vector<double> &s) { gmg.vmult(d, s); };
+  const double nr = norm2(rhs);
+  bool conv = true;
+  if (nr > 0) cg_solve(Am, Pm, lam, rhs, 100000, 1e-13 * nr, 0.0, &conv, nullptr, nullptr, nullptr);
+  if (!conv) return 3;
+  grad.assign(m.n_cells, 0.0);
+  dresidual_dlogmu_dot(m, bas, lmu[nl - 1], prm.nu, prm.formulation, u.data(), lam.data(), grad.data());
   return 0;
 }
 

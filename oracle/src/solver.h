@@ -80,6 +80,9 @@ struct StepResult {
   int newton_iterations = 0;
   bool converged = false;
   std::vector<int> cg_iterations;
+  // per Newton iteration: relative residual and relative update norm seen
+  // by the convergence check
+  std::vector<double> rel_res, rel_upd;
   double point_u[3] = {0, 0, 0};
 };
 
@@ -97,5 +100,9 @@ void setup_gmg(const NewtonParams &prm, const std::vector<Mesh> &meshes, const B
                const std::vector<std::vector<uint8_t>> &lmask, const std::vector<std::vector<double>> &lmu,
                const std::vector<double> &u_fine, GMG<LT> &gmg, bool first);
 int newton_run(const NewtonParams &prm, NewtonResult &res);
+// adjoint gradient of a boundary misfit with respect to the per-cell log
+// shear modulus (returns 0, or the newton_run / CG failure code)
+int adjoint_run(const NewtonParams &prm, const std::vector<double> &log_mu, const std::vector<double> &target,
+                int obj_id, double &J, std::vector<double> &grad, std::vector<double> &u);
 
 }  // namespace orc

@@ -1,8 +1,12 @@
 """Generate tests/golden/cook_3d_goldens.json from the reference's own
 integration-test goldens (tests/*.prm + tests/*.output of
-davydden/large-strain-matrix-free).  Run once in a container where the
-reference tree is mounted; the JSON it writes is committed so that the
-test-suite never reads the reference at run time.
+davydden/large-strain-matrix-free).  Run once where the reference tree is
+available, giving its root directory:
+
+    python tests/golden/make_golden.py <reference-root>
+
+The JSON it writes is committed so that the test-suite never reads the
+reference at run time.
 
 Only the numbers are extracted: mesh size, reference volume, Newton
 iteration counts and the displacement printed at the output point, plus the
@@ -13,7 +17,6 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 CASES = ["cook_3d_quad_mf", "cook_3d_lin_mf"]
 
 
@@ -42,12 +45,12 @@ def parse_output(text):
     return res
 
 
-def main():
+def main(ref_root):
     data = {}
     for c in CASES:
-        with open(os.path.join(REF, "tests", c + ".prm")) as f:
+        with open(os.path.join(ref_root, "tests", c + ".prm")) as f:
             prm = parse_prm(f.read())
-        with open(os.path.join(REF, "tests", c + ".output")) as f:
+        with open(os.path.join(ref_root, "tests", c + ".output")) as f:
             out = parse_output(f.read())
         data[c] = {"source": "tests/%s.prm + tests/%s.output" % (c, c), "prm": prm, "output": out}
     here = os.path.dirname(os.path.abspath(__file__))
@@ -56,4 +59,6 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference-root>")
+    main(sys.argv[1])

@@ -122,3 +122,38 @@ def test_gmg_matches_jacobi_solution():
     assert [s["newton_iterations"] for s in a["steps"]] == [s["newton_iterations"] for s in b["steps"]]
     assert np.max(np.abs(a["u"] - b["u"])) <= 1e-8 * np.max(np.abs(a["u"]))
     assert sum(s["cg_iterations"] for s in b["steps"]) < sum(s["cg_iterations"] for s in a["steps"]) / 5
+
+
+def _adjoint_kw(formulation):
+    # 4^3 Q2 box, bottom clamped, traction on the top face, solved tightly
+    return dict(geometry=O.GEOM_BOX, coarse=(2, 2, 2), n_refinements=1, p=2, q=3,
+                caching="tensor4" if formulation == 1 else "scalar", formulation=formulation, mu=1.0, nu=0.3,
+                dirichlet=[(4, 7, (0, 0, 0))], neumann=[(5, (0, 0, 0), (0.02, 0, -0.05))], end_time=1.0, dt=1.0,
+                tol_lin=1e-13, tol_f=1e-11, tol_u=1e-10, max_nr=25, precond="gmg", level_fp32=False)
+
+
+@pytest.mark.parametrize("formulation", [0, 1])
+def test_oracle_adjoint_gradient_matches_its_finite_differences(formulation):
+    """The oracle's FP64 adjoint gradient (tau differentiated in mu, adjoint
+    CG) against central differences of its own Newton solves: it is the
+    reference gradient the device adjoint is checked against."""
+    kw = _adjoint_kw(formulation)
+    m = O.Mesh(O.GEOM_BOX, (2, 2, 2), 1, (0, 0, 0), (1, 1, 1), 1.0, 2, 3)
+    rng = np.random.default_rng(17)
+    theta = rng.normal(0.0, 0.3, m.n_cells)
+    target = rng.uniform(-1e-3, 1e-3, m.n_dofs)
+    J, grad, u = O.adjoint(theta, target, 5, **kw)
+    assert J > 0 and np.all(np.isfinite(grad)) and np.max(np.abs(grad)) > 0
+    top = np.repeat(np.isclose(m.X[:, 2], 1.0), 3)
+    assert abs(J - 0.5 * np.sum((u[top] - target[top]) ** 2)) <= 1e-14 * J
+    h = 1e-6
+    fd, ad = [], []
+    for _ in range(4):
+        v = rng.normal(size=m.n_cells)
+        v /= np.linalg.norm(v)
+        jp = O.adjoint(theta + h * v, target, 5, **kw)[0]
+        jm = O.adjoint(theta - h * v, target, 5, **kw)[0]
+        fd.append((jp - jm) / (2 * h))
+        ad.append(grad @ v)
+    fd, ad = np.array(fd), np.array(ad)
+    assert np.max(np.abs(fd - ad)) <= 1e-6 * np.max(np.abs(fd)), (fd, ad)
