@@ -265,6 +265,48 @@ lsmf_status lsmf_problem_get_solution(const lsmf_problem *p, double *host_u);
  * expressions.  Waits for the problem's stream (norm is a host value). */
 lsmf_status lsmf_residual(lsmf_problem *p, const double *d_u, double t, double *d_R, double *norm);
 
+/* ---- z-slab partitions and the distributed operator ----
+ * The reference distributes its mesh over MPI ranks and exchanges the
+ * interface values around every cell loop (src.update_ghost_values(), cell
+ * loop, dst.compress(add): mf_nh_operator.h:680-700) and all-reduces the CG
+ * scalars (SolverCG, mf_elasticity.h:3175-3180).  Here part r of n_parts
+ * owns the coarse cell layers k in [floor(r nz / n), floor((r+1) nz / n)) of
+ * the structured mesh (with all refinements); the nodes of an interface
+ * plane are owned by the upper part.  Local vectors of a part hold its owned
+ * nodes and its ghost nodes (the upper interface), node-major. */
+lsmf_status lsmf_mesh_create_part(const lsmf_mesh_desc *desc, int n_parts, int part, lsmf_mesh **out);
+/* Host-only layout of a part (no device needed): its node count, the node
+ * count of the whole mesh, the whole-mesh node number of each local node,
+ * and the local nodes shared with part - 1 (owned here) and with part + 1
+ * (ghosts here), both in whole-mesh node order.  Output arrays may be NULL
+ * (sizes only). */
+lsmf_status lsmf_partition_layout(const lsmf_mesh_desc *desc, int n_parts, int part, int *n_nodes, int *n_global_nodes,
+                                  int *global_node, int *n_lower, int *lower, int *n_upper, int *upper);
+typedef struct lsmf_dist lsmf_dist;
+/* All parts in this process: ops[r] is the FP64 finest-level operator of
+ * part r; each part's work is ordered on its operator's stream, interface
+ * buffers move with cudaMemcpyAsync between the parts' streams. */
+lsmf_status lsmf_dist_create_group(int n_parts, lsmf_op *const *ops, lsmf_dist **out);
+/* One part per process over NCCL (libnccl.so.2 loaded at run time): every
+ * process passes the same 128-byte id, made by one of them with
+ * lsmf_dist_nccl_unique_id and shared by the host framework. */
+lsmf_status lsmf_dist_nccl_unique_id(unsigned char *id128);
+lsmf_status lsmf_dist_create_nccl(lsmf_op *op, const unsigned char *id128, lsmf_dist **out);
+void lsmf_dist_destroy(lsmf_dist *d);
+/* dst = A src over all parts (arrays of this object's local vectors, one
+ * per part it holds): ghost entries of src are set from their owners, the
+ * cell loops run, the ghosts' partial sums are added on the owners and the
+ * ghost entries of dst cleared.  dst is valid on the owned entries. */
+lsmf_status lsmf_dist_vmult(lsmf_dist *d, double *const *dst, double *const *src);
+/* sum over the owned entries of a . b, over all parts (host value) */
+lsmf_status lsmf_dist_dot(lsmf_dist *d, const double *const *a, const double *const *b, double *out);
+/* SolverCG over the parts, precond 0 (none) or 1 (Jacobi with the
+ * diagonal summed across the interfaces).  b: right-hand side on the owned
+ * entries (its ghost entries are ignored).  x: initial guess, solution on
+ * return (ghost entries set from their owners). */
+lsmf_status lsmf_dist_cg_solve(lsmf_dist *d, int precond, double omega, double *const *x, const double *const *b,
+                               double tol_abs, int max_it, lsmf_solve_info *info);
+
 /* ---- allocation-free residual norm (no counterpart in the reference) ----
  * *d_norm = ||d_b - A d_x||_2 for a cached FP64 operator, computed without
  * calling cudaMalloc: for callers that cannot allocate device memory while

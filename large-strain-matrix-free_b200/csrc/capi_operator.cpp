@@ -58,6 +58,60 @@ lsmf_status lsmf_mesh_create(const lsmf_mesh_desc *desc, lsmf_mesh **out) {
   return LSMF_OK;
 }
 
+// the coarse z-cells [k0, k1) of part `part` of n_parts: as even as possible
+static void slab_range(int nz, int n_parts, int part, int &k0, int &k1) {
+  k0 = (int)((long long)nz * part / n_parts);
+  k1 = (int)((long long)nz * (part + 1) / n_parts);
+}
+
+static lsmf_status make_part_mesh(const lsmf_mesh_desc *desc, int n_parts, int part, bool host_only, lsmf_mesh **out) {
+  if (!desc || !out) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  *out = nullptr;
+  if (n_parts < 1 || part < 0 || part >= n_parts) { set_error("bad part / n_parts"); return LSMF_ERR_INVALID_ARG; }
+  if (desc->coarse[2] < n_parts) {
+    set_error("a partition needs at least one coarse cell layer in z per part");
+    return LSMF_ERR_INVALID_ARG;
+  }
+  lsmf_mesh *m = new (std::nothrow) lsmf_mesh();
+  if (!m) return LSMF_ERR_ALLOC;
+  m->desc = *desc;
+  if (desc->coarse_active) {
+    const size_t n = (size_t)desc->coarse[0] * desc->coarse[1] * desc->coarse[2];
+    m->coarse_active.assign(desc->coarse_active, desc->coarse_active + n);
+  }
+  m->desc.coarse_active = nullptr;
+  m->host_only = host_only;
+  m->layout.n_parts = n_parts;
+  m->layout.part = part;
+  slab_range(desc->coarse[2], n_parts, part, m->layout.k0, m->layout.k1);
+  lsmf_status s = build_mesh(*m);
+  if (s != LSMF_OK) { delete m; return s; }
+  *out = m;
+  return LSMF_OK;
+}
+
+lsmf_status lsmf_mesh_create_part(const lsmf_mesh_desc *desc, int n_parts, int part, lsmf_mesh **out) {
+  return make_part_mesh(desc, n_parts, part, false, out);
+}
+
+lsmf_status lsmf_partition_layout(const lsmf_mesh_desc *desc, int n_parts, int part, int *n_nodes, int *n_global_nodes,
+                                  int *global_node, int *n_lower, int *lower, int *n_upper, int *upper) {
+  lsmf_mesh *m = nullptr;
+  LSMF_TRY(make_part_mesh(desc, n_parts, part, true, &m));
+  const PartLayout &P = m->layout;
+  const int nn = m->levels.back()->n_nodes;
+  if (n_nodes) *n_nodes = nn;
+  if (n_global_nodes) *n_global_nodes = n_parts > 1 ? P.n_global_nodes : nn;
+  if (global_node)
+    for (int i = 0; i < nn; ++i) global_node[i] = n_parts > 1 ? P.global_node[i] : i;
+  if (n_lower) *n_lower = (int)P.lower_shared.size();
+  if (lower) std::memcpy(lower, P.lower_shared.data(), P.lower_shared.size() * sizeof(int));
+  if (n_upper) *n_upper = (int)P.upper_shared.size();
+  if (upper) std::memcpy(upper, P.upper_shared.data(), P.upper_shared.size() * sizeof(int));
+  delete m;
+  return LSMF_OK;
+}
+
 void lsmf_mesh_destroy(lsmf_mesh *m) { delete m; }
 
 int lsmf_mesh_n_levels(const lsmf_mesh *m) { return m ? (int)m->levels.size() : 0; }

@@ -123,11 +123,31 @@ struct TransferMap {
   DevBuf<double> d_interp_w;           // per coarse node: (p+1)^3 weights
 };
 
+// Layout of one z-slab partition of the finest level: the part owns the
+// coarse cells with k in [k0, k1) (all their refinements).  Local nodes are
+// numbered in lattice order like the whole mesh, so both parts of an
+// interface list its shared nodes in the same (global) order.  The shared
+// nodes of an interface plane are owned by the upper part: upper_shared are
+// this part's ghosts (their values live on part + 1), lower_shared are owned
+// here and are ghosts of part - 1.
+struct PartLayout {
+  int n_parts = 1, part = 0, k0 = 0, k1 = 0;
+  std::vector<int> global_node;   // local node -> node of the whole mesh
+  std::vector<int> lower_shared;  // local nodes shared with part - 1
+  std::vector<int> upper_shared;  // local nodes shared with part + 1
+  int n_global_nodes = 0;
+};
+
 }  // namespace lsmf
 
 struct lsmf_mesh {
   lsmf_mesh_desc desc{};
   std::vector<uint8_t> coarse_active;
+  // z-slab partition (n_parts == 1: the whole mesh)
+  lsmf::PartLayout layout;
+  // build the host-side levels and layout only (no device buffers, no
+  // constraints or transfers): the partition query needs no GPU
+  bool host_only = false;
   lsmf::Basis basis;
   std::vector<lsmf::Level *> levels;          // 0 = coarsest
   std::vector<lsmf::TransferMap *> transfer;  // transfer[l] : l-1 -> l (l>=1)

@@ -105,11 +105,20 @@ void build_level(const lsmf_mesh &M, int level, Level &L) {
   L.p = p; L.q = d.n_q_points_1d;
   for (int k = 0; k < 3; ++k) { L.nc[k] = d.coarse[k] << level; L.nn[k] = p * L.nc[k] + 1; }
   const int ncx = L.nc[0], ncy = L.nc[1], ncz = L.nc[2];
+  // active: a cell of the whole mesh; member: a cell of this mesh (of its
+  // z-slab when the mesh is one part of a partition).  Faces between two
+  // active cells are interior, also across a partition interface.
   auto active = [&](int i, int j, int k) {
     if (i < 0 || j < 0 || k < 0 || i >= ncx || j >= ncy || k >= ncz) return false;
     if (M.coarse_active.empty()) return true;
     const int ci = i >> level, cj = j >> level, ck = k >> level;
     return M.coarse_active[(size_t)(ck * d.coarse[1] + cj) * d.coarse[0] + ci] != 0;
+  };
+  auto member = [&](int i, int j, int k) {
+    if (!active(i, j, k)) return false;
+    if (M.layout.n_parts <= 1) return true;
+    const int ck = k >> level;
+    return ck >= M.layout.k0 && ck < M.layout.k1;
   };
   const size_t nlat = (size_t)L.nn[0] * L.nn[1] * L.nn[2];
   L.lattice_to_node.assign(nlat, -1);
@@ -117,7 +126,7 @@ void build_level(const lsmf_mesh &M, int level, Level &L) {
   for (int k = 0; k < ncz; ++k)
     for (int j = 0; j < ncy; ++j)
       for (int i = 0; i < ncx; ++i) {
-        if (!active(i, j, k)) continue;
+        if (!member(i, j, k)) continue;
         L.cell_of_lattice[((size_t)k * ncy + j) * ncx + i] = L.n_cells++;
         L.cell_ijk.insert(L.cell_ijk.end(), {i, j, k});
         for (int c = 0; c <= p; ++c)
@@ -280,6 +289,51 @@ static lsmf_status build_transfer(const lsmf_mesh &M, const Level &C, const Leve
   return LSMF_OK;
 }
 
+// Global node numbers and interface lists of a z-slab part on the finest
+// level L (see PartLayout).  A lattice point is a node of the whole mesh when
+// an active cell touches it; the whole mesh numbers its nodes in lattice
+// order, so a prefix count over the lattice gives the global numbers.
+static void build_layout(lsmf_mesh &M, const Level &L, int level) {
+  PartLayout &P = M.layout;
+  const lsmf_mesh_desc &d = M.desc;
+  const int p = L.p, ncx = L.nc[0], ncy = L.nc[1], ncz = L.nc[2];
+  auto active = [&](int i, int j, int k) {
+    if (i < 0 || j < 0 || k < 0 || i >= ncx || j >= ncy || k >= ncz) return false;
+    if (M.coarse_active.empty()) return true;
+    return M.coarse_active[(size_t)((k >> level) * d.coarse[1] + (j >> level)) * d.coarse[0] + (i >> level)] != 0;
+  };
+  // cells of layer k touching lattice point (a, b) of a z-plane
+  auto touches_layer = [&](int a, int b, int k) {
+    const int ia[2] = {a % p == 0 ? a / p - 1 : a / p, a / p};
+    const int jb[2] = {b % p == 0 ? b / p - 1 : b / p, b / p};
+    for (int s = 0; s < 2; ++s)
+      for (int t = 0; t < 2; ++t)
+        if (active(ia[s], jb[t], k)) return true;
+    return false;
+  };
+  const size_t nlat = (size_t)L.nn[0] * L.nn[1] * L.nn[2];
+  std::vector<int> gnum(nlat, -1);
+  int g = 0;
+  const size_t plane = (size_t)L.nn[0] * L.nn[1];
+  for (size_t l = 0; l < nlat; ++l) {
+    const int a = (int)(l % L.nn[0]), b = (int)((l / L.nn[0]) % L.nn[1]), c = (int)(l / plane);
+    const int ks[2] = {c % p == 0 ? c / p - 1 : c / p, c / p};
+    if (touches_layer(a, b, ks[0]) || (ks[1] != ks[0] && touches_layer(a, b, ks[1]))) gnum[l] = g++;
+  }
+  P.n_global_nodes = g;
+  P.global_node.resize(L.n_nodes);
+  P.lower_shared.clear();
+  P.upper_shared.clear();
+  const int zlo = P.k0 * (1 << level) * p, zhi = P.k1 * (1 << level) * p;
+  for (int n = 0; n < L.n_nodes; ++n) {
+    const size_t l = L.node_lattice[n];
+    P.global_node[n] = gnum[l];
+    const int a = (int)(l % L.nn[0]), b = (int)((l / L.nn[0]) % L.nn[1]), c = (int)(l / plane);
+    if (P.part > 0 && c == zlo && touches_layer(a, b, zlo / p - 1)) P.lower_shared.push_back(n);
+    if (P.part < P.n_parts - 1 && c == zhi && touches_layer(a, b, zhi / p)) P.upper_shared.push_back(n);
+  }
+}
+
 lsmf_status build_mesh(lsmf_mesh &M) {
   const lsmf_mesh_desc &d = M.desc;
   if (d.degree < 1 || d.degree > 4 || d.n_q_points_1d != d.degree + 1) {
@@ -296,6 +350,7 @@ lsmf_status build_mesh(lsmf_mesh &M) {
     M.levels.push_back(L);
     build_level(M, l, *L);
     if ((long long)L->n_nodes >= (1LL << NODE_BITS)) { set_error("too many nodes"); return LSMF_ERR_UNSUPPORTED; }
+    if (M.host_only) continue;
     LSMF_TRY(L->d_X.upload(L->X.data(), L->X.size()));
     LSMF_TRY(level_constraints(M, *L));
     // cells by lattice colour: two cells of one colour are two or more
@@ -312,10 +367,11 @@ lsmf_status build_mesh(lsmf_mesh &M) {
     LSMF_TRY(L->d_colour_cells.upload(L->colour_cells.data(), L->colour_cells.size()));
   }
   M.transfer.assign(nl, nullptr);
-  for (int l = 1; l < nl; ++l) {
+  for (int l = 1; l < nl && !M.host_only; ++l) {
     M.transfer[l] = new TransferMap();
     LSMF_TRY(build_transfer(M, *M.levels[l - 1], *M.levels[l], *M.transfer[l]));
   }
+  if (M.layout.n_parts > 1) build_layout(M, *M.levels[nl - 1], nl - 1);
   return LSMF_OK;
 }
 

@@ -110,6 +110,17 @@ SIGNATURES = {
     "lsmf_adjoint_forward": (ctypes.c_int, [vp, dp, dp, ctypes.c_int, dp]),
     "lsmf_adjoint_backward": (ctypes.c_int, [vp, dp]),
     "lsmf_residual_norm_noalloc": (ctypes.c_int, [vp, vp, vp, vp]),
+    "lsmf_mesh_create_part": (ctypes.c_int, [ctypes.POINTER(MeshDesc), ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]),
+    "lsmf_partition_layout": (ctypes.c_int, [ctypes.POINTER(MeshDesc), ctypes.c_int, ctypes.c_int, ip, ip, vp, ip, vp,
+                                             ip, vp]),
+    "lsmf_dist_create_group": (ctypes.c_int, [ctypes.c_int, vp, ctypes.POINTER(vp)]),
+    "lsmf_dist_nccl_unique_id": (ctypes.c_int, [vp]),
+    "lsmf_dist_create_nccl": (ctypes.c_int, [vp, vp, ctypes.POINTER(vp)]),
+    "lsmf_dist_destroy": (None, [vp]),
+    "lsmf_dist_vmult": (ctypes.c_int, [vp, vp, vp]),
+    "lsmf_dist_dot": (ctypes.c_int, [vp, vp, vp, dp]),
+    "lsmf_dist_cg_solve": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, vp, vp, ctypes.c_double, ctypes.c_int,
+                                          ctypes.POINTER(SolveInfo)]),
 }
 
 
@@ -152,23 +163,54 @@ def _dptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
+def _mesh_desc(geometry="box", coarse=(1, 1, 1), n_refinements=0, lo=(0, 0, 0), hi=(1, 1, 1), scale=1.0, degree=2,
+               n_q_points_1d=None, coarse_active=None):
+    """lsmf_mesh_desc and the mask array it points to (kept alive by the caller)."""
+    d = MeshDesc()
+    d.geometry = GEOM[geometry] if isinstance(geometry, str) else int(geometry)
+    for k in range(3):
+        d.coarse[k], d.lo[k], d.hi[k] = coarse[k], lo[k], hi[k]
+    d.n_refinements, d.scale, d.degree = n_refinements, scale, degree
+    d.n_q_points_1d = degree + 1 if n_q_points_1d is None else n_q_points_1d
+    mask = None
+    if coarse_active is not None:
+        mask = np.ascontiguousarray(coarse_active, dtype=np.uint8)
+        d.coarse_active = mask.ctypes.data
+    return d, mask
+
+
+def partition_layout(n_parts, part, **mesh_kw):
+    """Host-only layout of z-slab part `part` of `n_parts` (no GPU needed):
+    whole-mesh node number of each local node, the local nodes shared with
+    part - 1 (owned here) and with part + 1 (ghosts here)."""
+    d, mask = _mesh_desc(**mesh_kw)
+    nn, ng, nlo, nup = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    check(lib().lsmf_partition_layout(ctypes.byref(d), n_parts, part, ctypes.byref(nn), ctypes.byref(ng), None,
+                                      ctypes.byref(nlo), None, ctypes.byref(nup), None))
+    gn = np.zeros(nn.value, dtype=np.int32)
+    lo_ = np.zeros(max(1, nlo.value), dtype=np.int32)
+    up_ = np.zeros(max(1, nup.value), dtype=np.int32)
+    check(lib().lsmf_partition_layout(ctypes.byref(d), n_parts, part, ctypes.byref(nn), ctypes.byref(ng),
+                                      gn.ctypes.data, ctypes.byref(nlo), lo_.ctypes.data, ctypes.byref(nup),
+                                      up_.ctypes.data))
+    del mask
+    return {"n_nodes": nn.value, "n_global_nodes": ng.value, "global_node": gn,
+            "lower_shared": lo_[:nlo.value].copy(), "upper_shared": up_[:nup.value].copy()}
+
+
 class Mesh:
-    """Structured hex mesh hierarchy (levels 0..n_refinements)."""
+    """Structured hex mesh hierarchy (levels 0..n_refinements); with
+    n_parts > 1 the z-slab part `part` of that partition."""
 
     def __init__(self, geometry="box", coarse=(1, 1, 1), n_refinements=0, lo=(0, 0, 0), hi=(1, 1, 1),
-                 scale=1.0, degree=2, n_q_points_1d=None, coarse_active=None):
-        d = MeshDesc()
-        d.geometry = GEOM[geometry] if isinstance(geometry, str) else int(geometry)
-        for k in range(3):
-            d.coarse[k], d.lo[k], d.hi[k] = coarse[k], lo[k], hi[k]
-        d.n_refinements, d.scale, d.degree = n_refinements, scale, degree
-        d.n_q_points_1d = degree + 1 if n_q_points_1d is None else n_q_points_1d
-        self._mask = None
-        if coarse_active is not None:
-            self._mask = np.ascontiguousarray(coarse_active, dtype=np.uint8)
-            d.coarse_active = self._mask.ctypes.data
+                 scale=1.0, degree=2, n_q_points_1d=None, coarse_active=None, n_parts=1, part=0):
+        d, self._mask = _mesh_desc(geometry, coarse, n_refinements, lo, hi, scale, degree, n_q_points_1d,
+                                   coarse_active)
         h = vp()
-        check(lib().lsmf_mesh_create(ctypes.byref(d), ctypes.byref(h)))
+        if n_parts > 1:
+            check(lib().lsmf_mesh_create_part(ctypes.byref(d), n_parts, part, ctypes.byref(h)))
+        else:
+            check(lib().lsmf_mesh_create(ctypes.byref(d), ctypes.byref(h)))
         self._L = lib()
         self.h = h
         self.degree = degree
@@ -384,6 +426,67 @@ def cg_solve(op, x, b, tol, max_it, precond="gmg", gmg=None, omega=1.0):
         check(st)
     return {"iterations": info.iterations, "residual": info.residual, "converged": bool(info.converged),
             "status": st}
+
+
+def _ptr_array(tensors):
+    arr = (ctypes.c_void_p * len(tensors))(*[_dptr(t).value for t in tensors])
+    return arr
+
+
+class Dist:
+    """The distributed operator over z-slab parts (update_ghost_values, cell
+    loop, compress(add) around every vmult; all-reduced CG scalars).  Build
+    it with group(ops) (all parts in this process) or nccl(op, id) (one part
+    per process).  Vectors are lists of the local vectors of the parts this
+    object holds (one tensor for nccl)."""
+
+    def __init__(self, h, n_local):
+        self._L = lib()
+        self.h, self.n_local = h, n_local
+
+    @classmethod
+    def group(cls, ops):
+        h = vp()
+        arr = (ctypes.c_void_p * len(ops))(*[o.h.value for o in ops])
+        check(lib().lsmf_dist_create_group(len(ops), arr, ctypes.byref(h)))
+        obj = cls(h, len(ops))
+        obj._ops = list(ops)
+        return obj
+
+    @staticmethod
+    def nccl_unique_id():
+        buf = (ctypes.c_ubyte * 128)()
+        check(lib().lsmf_dist_nccl_unique_id(buf))
+        return bytes(buf)
+
+    @classmethod
+    def nccl(cls, op, uid):
+        h = vp()
+        buf = (ctypes.c_ubyte * 128).from_buffer_copy(uid)
+        check(lib().lsmf_dist_create_nccl(op.h, buf, ctypes.byref(h)))
+        obj = cls(h, 1)
+        obj._ops = [op]
+        return obj
+
+    def __del__(self, _release=_release):  # bound now: module globals are gone at exit
+        _release(self, "lsmf_dist_destroy")
+
+    def vmult(self, dsts, srcs):
+        check(lib().lsmf_dist_vmult(self.h, _ptr_array(dsts), _ptr_array(srcs)))
+
+    def dot(self, a, b):
+        out = ctypes.c_double()
+        check(lib().lsmf_dist_dot(self.h, _ptr_array(a), _ptr_array(b), ctypes.byref(out)))
+        return out.value
+
+    def cg_solve(self, xs, bs, tol, max_it, precond="jacobi", omega=1.0):
+        info = SolveInfo()
+        st = lib().lsmf_dist_cg_solve(self.h, {"none": 0, "jacobi": 1}[precond], omega, _ptr_array(xs),
+                                      _ptr_array(bs), tol, max_it, ctypes.byref(info))
+        if st not in (0, 5):
+            check(st)
+        return {"iterations": info.iterations, "residual": info.residual, "converged": bool(info.converged),
+                "status": st}
 
 
 def prm_validate(prm_text):

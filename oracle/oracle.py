@@ -211,6 +211,54 @@ def residual(mesh, mu_cell, nu, formulation, u, neumann, time, cmask):
     return R, nrm
 
 
+def assemble_tangent(mesh, mu_cell, nu, formulation, u, cmask):
+    """The matrix-based tangent of the whole mesh (FEValues-style element
+    matrices summed, constrained rows and columns an identity block) as a
+    scipy CSR matrix."""
+    import scipy.sparse as sp
+    L = lib()
+    L.orc_assemble_coo.restype = ctypes.c_long
+    mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu_cell, dtype=np.float64), (mesh.n_cells,)))
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    cm = np.ascontiguousarray(cmask, dtype=np.uint8)
+    args = [mesh.h, _p(mu), ctypes.c_double(nu), ctypes.c_int(formulation), _p(u), _p(cm)]
+    n = L.orc_assemble_coo(*args, None, None, None)
+    rows, cols, vals = np.zeros(n, dtype=np.int32), np.zeros(n, dtype=np.int32), np.zeros(n)
+    L.orc_assemble_coo(*args, _p(rows), _p(cols), _p(vals))
+    keep = rows >= 0
+    return sp.csr_matrix((vals[keep], (rows[keep], cols[keep])), shape=(mesh.n_dofs, mesh.n_dofs))
+
+
+def cg_jacobi(K, b, tol_abs, max_it, omega=1.0):
+    """deal.II SolverCG with PreconditionJacobi (omega D^-1) on an assembled
+    matrix: g = K x - b, convergence on ||g|| <= tol_abs from x = 0.  Returns
+    (x, iterations, converged)."""
+    invd = omega / K.diagonal()
+    x = np.zeros_like(b)
+    g = -b.copy()
+    res = np.linalg.norm(g)
+    if res <= tol_abs:
+        return x, 0, True
+    h = invd * g
+    d = -h
+    gh = g @ h
+    it = 0
+    while it < max_it:
+        it += 1
+        h = K @ d
+        alpha = gh / (d @ h)
+        x += alpha * d
+        g += alpha * h
+        res = np.linalg.norm(g)
+        if res <= tol_abs:
+            return x, it, True
+        h = invd * g
+        gh_new = g @ h
+        d = -h + (gh_new / gh) * d
+        gh = gh_new
+    return x, it, False
+
+
 def element_matrix(mesh, cell, mu, nu, formulation, u):
     nd = 3 * (mesh.p + 1) ** 3
     K = np.zeros((nd, nd))

@@ -158,6 +158,47 @@ void orc_element_matrix(void *mh, int cell, double mu, double nu, int formulatio
   std::memcpy(K, k.data(), sizeof(double) * k.size());
 }
 
+// Matrix-based tangent of the whole mesh (assemble_system's tangent part,
+// mf_elasticity.h:2760-2843, through the FEValues-style element matrices)
+// as COO triplets: slot range [cell * ND^2, (cell + 1) * ND^2) holds cell's
+// entries, with row = -1 where a constrained row or column is dropped; then
+// one unit diagonal entry per constrained dof (AffineConstraints keep the
+// constrained rows and columns of the system matrix as an identity block,
+// which is what the matrix-free operator applies).  Returns the slot count;
+// with rows == nullptr only the count.
+long orc_assemble_coo(void *mh, const double *mu_cell, double nu, int formulation, const double *u,
+                      const unsigned char *cmask, int *rows, int *cols, double *vals) {
+  auto *h = (MeshH *)mh;
+  const Mesh &m = h->m;
+  const int NN = m.ncn(), ND = 3 * NN;
+  long n_con = 0;
+  for (int i = 0; i < m.n_dofs(); ++i) n_con += cmask[i] ? 1 : 0;
+  const long total = (long)m.n_cells * ND * ND + n_con;
+  if (!rows) return total;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int cell = 0; cell < m.n_cells; ++cell) {
+    std::vector<double> K;
+    element_matrix(m, h->b, cell, Material(mu_cell[cell], nu, formulation), u, K);
+    const int *nodes = &m.cell_nodes[(size_t)cell * NN];
+    const long base = (long)cell * ND * ND;
+    for (int i = 0; i < ND; ++i) {
+      const int gi = 3 * nodes[i % NN] + i / NN;
+      for (int j = 0; j < ND; ++j) {
+        const int gj = 3 * nodes[j % NN] + j / NN;
+        const long s = base + (long)i * ND + j;
+        const bool keep = !cmask[gi] && !cmask[gj];
+        rows[s] = keep ? gi : -1;
+        cols[s] = gj;
+        vals[s] = K[(size_t)i * ND + j];
+      }
+    }
+  }
+  long s = (long)m.n_cells * ND * ND;
+  for (int i = 0; i < m.n_dofs(); ++i)
+    if (cmask[i]) { rows[s] = i; cols[s] = i; vals[s] = 1.0; ++s; }
+  return total;
+}
+
 // ------------------------------------------------------------ transfer
 struct TrH { Transfer t; MeshH *c, *f; };
 void *orc_transfer_new(void *coarse, void *fine) {

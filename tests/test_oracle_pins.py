@@ -157,3 +157,28 @@ def test_oracle_adjoint_gradient_matches_its_finite_differences(formulation):
         ad.append(grad @ v)
     fd, ad = np.array(fd), np.array(ad)
     assert np.max(np.abs(fd - ad)) <= 1e-6 * np.max(np.abs(fd)), (fd, ad)
+
+
+@pytest.mark.parametrize("formulation,caching", [(1, "tensor4"), (0, "scalar"), (1, "tensor4_ns")])
+def test_matrix_based_tangent_equals_matrix_free_operator(formulation, caching):
+    """The reference's test method (matrix-free cell action = FEValues element
+    matrix, tests/mf_neo_hook_operator.cc) on a whole 4^3 Q2 mesh with
+    constraints: the assembled tangent times a vector equals the oracle's
+    matrix-free vmult, and Jacobi-CG on the matrix converges like CG on the
+    matrix-free operator (same iterations)."""
+    m = O.Mesh(O.GEOM_BOX, (2, 2, 2), 1, (0, 0, 0), (1, 1, 1), 1.0, 2, 3)
+    cm = m.constraints([(4, 7), (5, 4)])
+    rng = np.random.default_rng(9)
+    mu = rng.choice([1.0, 10.0], m.n_cells)
+    u = 0.01 * np.sin(np.pi * m.X[:, [1, 2, 0]]).reshape(-1)
+    K = O.assemble_tangent(m, mu, 0.3, formulation, u, cm)
+    op = O.Operator(m, caching, formulation)
+    op.set_material(mu, 0.3)
+    op.set_constraints(cm)
+    op.cache(u)
+    x = rng.uniform(-1, 1, m.n_dofs)
+    assert np.max(np.abs(K @ x - op.vmult(x))) <= 1e-10 * np.max(np.abs(op.vmult(x)))
+    assert abs((K - K.T).max()) <= 1e-10 * abs(K).max()     # the tangent is symmetric
+    b = np.where(cm == 1, 0.0, rng.uniform(-1, 1, m.n_dofs))
+    xk, itk, ok = O.cg_jacobi(K, b, 1e-10 * np.linalg.norm(b), 5000)
+    assert ok and np.linalg.norm(op.vmult(xk) - b) <= 1.01e-10 * np.linalg.norm(b)
