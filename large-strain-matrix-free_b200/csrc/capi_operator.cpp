@@ -181,8 +181,20 @@ lsmf_status lsmf_operator_create(lsmf_mesh *m, int level, lsmf_caching caching, 
   if (cudaGetDevice(&op->device) != cudaSuccess) { delete op; set_error("cudaGetDevice failed"); return LSMF_ERR_CUDA; }
   op->ncomp = table_components(caching, formulation, precision);
   const Level &L = op->L();
+  // scalar caching on affine cells: the reference inverse Jacobian is one
+  // 3x3 block per cell after the 11 per-point values (c, Eulerian inverse
+  // Jacobian, JxW), the record padded to 16 bytes; otherwise ncomp values
+  // per point
+  op->ref_per_cell = caching == LSMF_CACHE_SCALAR && L.affine;
+  if (op->ref_per_cell) {
+    op->ncomp = 11;
+    const int al = 16 / (int)op->elem();
+    op->rec_elems = (11 * L.nq() + 9 + al - 1) / al * al;
+  } else {
+    op->rec_elems = op->ncomp * L.nq();
+  }
   lsmf_status s;
-  if ((s = op->d_table.alloc((size_t)L.n_cells * op->ncomp * L.nq() * op->elem())) != LSMF_OK ||
+  if ((s = op->d_table.alloc((size_t)L.n_cells * op->rec_elems * op->elem())) != LSMF_OK ||
       (s = op->d_diag.alloc((size_t)L.n_dofs() * op->elem())) != LSMF_OK ||
       (s = op->d_inv_diag.alloc((size_t)L.n_dofs() * op->elem())) != LSMF_OK ||
       (s = op->d_flag.alloc(1)) != LSMF_OK) {
@@ -343,7 +355,7 @@ size_t lsmf_operator_memory_consumption(const lsmf_op *op) {
 lsmf_status lsmf_operator_get_table(lsmf_op *op, int which, double *host, size_t *count) {
   if (!op || !count) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
   const Level &L = op->L();
-  const int nq = L.nq(), nc = op->ncomp;
+  const int nq = L.nq();
   int c0 = 0, nk = 0;
   const bool t4 = op->caching == LSMF_CACHE_TENSOR4, t2 = op->caching == LSMF_CACHE_TENSOR2;
   const bool sr = op->caching == LSMF_CACHE_SCALAR_REFERENTIAL, ns = op->caching == LSMF_CACHE_TENSOR4_NS;
@@ -367,7 +379,7 @@ lsmf_status lsmf_operator_get_table(lsmf_op *op, int which, double *host, size_t
   for (int cell = 0; cell < L.n_cells; ++cell)
     for (int q = 0; q < nq; ++q)
       for (int k = 0; k < nk; ++k) {
-        const size_t src = ((size_t)cell * nc + c0 + k) * nq + q;
+        const size_t src = (size_t)cell * op->rec_elems + (size_t)(c0 + k) * nq + q;
         const double v = op->precision == LSMF_FP64 ? ((const double *)raw.data())[src]
                                                     : (double)((const float *)raw.data())[src];
         host[((size_t)cell * nq + q) * nk + k] = v;

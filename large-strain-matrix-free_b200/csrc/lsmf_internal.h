@@ -86,6 +86,7 @@ struct Level {
   int p = 2, q = 3;
   int nc[3] = {0, 0, 0}, nn[3] = {0, 0, 0};
   int n_cells = 0, n_nodes = 0;
+  bool affine = false;          // every cell an affine image of the unit cube (box meshes)
   std::vector<int> lattice_to_node, node_lattice, cell_of_lattice;
   std::vector<double> X;
   std::vector<int> cell_nodes;  // raw node ids
@@ -161,6 +162,8 @@ struct lsmf_op {
   int caching = LSMF_CACHE_TENSOR4, formulation = 1;
   lsmf_precision precision = LSMF_FP64;
   int ncomp = 0;                     // table components per qp
+  int rec_elems = 0;                 // values per cell record (ncomp * nq, plus per-cell values and padding)
+  bool ref_per_cell = false;         // scalar caching on affine cells: reference metric once per cell
   double nu = 0.3;
   std::vector<double> mu_host;
   lsmf::DevBuf<double> d_mu;         // per cell

@@ -103,6 +103,9 @@ void build_level(const lsmf_mesh &M, int level, Level &L) {
   const lsmf_mesh_desc &d = M.desc;
   const int p = d.degree;
   L.p = p; L.q = d.n_q_points_1d;
+  // axis-aligned box cells have a constant reference Jacobian; the Cook
+  // transformation bends them
+  L.affine = d.geometry == LSMF_GEOM_BOX;
   for (int k = 0; k < 3; ++k) { L.nc[k] = d.coarse[k] << level; L.nn[k] = p * L.nc[k] + 1; }
   const int ncx = L.nc[0], ncy = L.nc[1], ncz = L.nc[2];
   // active: a cell of the whole mesh; member: a cell of this mesh (of its

@@ -28,6 +28,8 @@ struct KArgs {
   const int *cell_nodes;
   int n_cells;
   int ncomp;
+  int rec_elems;         // values per cell record
+  int ref_per_cell;      // scalar caching: reference inverse Jacobian once per cell
   T *table;              // cache records (written by cache, read by apply/diag)
   const T *src;
   T *dst;
@@ -164,7 +166,7 @@ __global__ void __launch_bounds__(256) cache_kernel(KArgs<T> a, Tab<P, Q> tab) {
     S::eval(sN, sD, V, A, B, lane, GU);
     const double mu = a.mu[cell];
     const double lambda = (2.0 * mu * a.nu) / (1.0 - 2.0 * a.nu);
-    T *rec = a.table + (size_t)cell * a.ncomp * NQ;
+    T *rec = a.table + (size_t)cell * a.rec_elems;
 #pragma unroll
     for (int l = 0; l < QPL; ++l) {
       const int q = lane + 32 * l;
@@ -204,8 +206,15 @@ __global__ void __launch_bounds__(256) cache_kernel(KArgs<T> a, Tab<P, Q> tab) {
       if (VAR == VAR_SCALAR_F0 || VAR == VAR_SCALAR_F1) {
         const double c = (VAR == VAR_SCALAR_F0) ? pow(det_F, -1.0 / 3.0) : mu - 2.0 * lambda * log(det_F);
         r[C_VAR * NQ] = T(c);
+        if (a.ref_per_cell) {
+          // affine cell: the reference metric of the first point stands for all
+          if (q == 0)
 #pragma unroll
-        for (int i = 0; i < 9; ++i) r[(C_VAR + 1 + i) * NQ] = T(Jri[i / 3][i % 3]);
+            for (int i = 0; i < 9; ++i) rec[(C_VAR + 1) * NQ + i] = T(Jri[i / 3][i % 3]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 9; ++i) r[(C_VAR + 1 + i) * NQ] = T(Jri[i / 3][i % 3]);
+        }
         continue;
       }
       const double scalar = mu - 2.0 * lambda * log(det_F);
@@ -291,7 +300,7 @@ __global__ void __launch_bounds__(256) apply_kernel(KArgs<T> a, Tab<P, Q> tab) {
   for (int ic = gw; ic < a.n_cells; ic += nw) {
     const int cell = cell_of(a, ic);
     const int *cn = a.cell_nodes + (size_t)cell * NN;
-    const T *rec = a.table + (size_t)cell * a.ncomp * NQ;
+    const T *rec = a.table + (size_t)cell * a.rec_elems;
     T G[QPL][3][3], GU[QPL][3][3];
     if (SCALAR) {
       if (rw) gather<NN>(cn, a.u, false, V, lane);   // read_dof_values_plain(u)
@@ -336,7 +345,8 @@ __global__ void __launch_bounds__(256) apply_kernel(KArgs<T> a, Tab<P, Q> tab) {
       if (SCALAR) {
         T Jr[3][3];
 #pragma unroll
-        for (int i = 0; i < 9; ++i) Jr[i / 3][i % 3] = r[(C_VAR + 1 + i) * NQ];
+        for (int i = 0; i < 9; ++i)
+          Jr[i / 3][i % 3] = a.ref_per_cell ? rec[(C_VAR + 1) * NQ + i] : r[(C_VAR + 1 + i) * NQ];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -406,7 +416,7 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
   constexpr bool PT_SMEM = !SCALAR && QPL >= 2;
   const int WPB = blockDim.x >> 5;
   extern __shared__ __align__(128) unsigned char smem[];
-  const int rec_elems = a.ncomp * NQ;
+  const int rec_elems = a.rec_elems;
   const uint32_t rec_bytes = (uint32_t)(rec_elems * sizeof(T));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t warp_bytes = ((STAGES * (size_t)rec_bytes + 8 * (STAGES > 0 ? STAGES : 1) + S::SZ * sizeof(T) + 127) / 128) * 128;
@@ -544,7 +554,8 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
       if (SCALAR) {
         T Jr[3][3];
 #pragma unroll
-        for (int i = 0; i < 9; ++i) Jr[i / 3][i % 3] = r[(C_VAR + 1 + i) * NQ];
+        for (int i = 0; i < 9; ++i)
+          Jr[i / 3][i % 3] = a.ref_per_cell ? rec[(C_VAR + 1) * NQ + i] : r[(C_VAR + 1 + i) * NQ];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -625,7 +636,7 @@ __global__ void __launch_bounds__(128) diagonal_kernel(KArgs<T> a, Tab<P, Q> tab
   for (int ic = gw; ic < a.n_cells; ic += nw) {
     const int cell = cell_of(a, ic);
     const int *cn = a.cell_nodes + (size_t)cell * NN;
-    const T *rec = a.table + (size_t)cell * a.ncomp * NQ;
+    const T *rec = a.table + (size_t)cell * a.rec_elems;
     T GU[QPL][3][3];
     if (SCALAR) {
       gather<NN>(cn, a.u, false, V, lane);
@@ -649,7 +660,8 @@ __global__ void __launch_bounds__(128) diagonal_kernel(KArgs<T> a, Tab<P, Q> tab
       if (SCALAR) {
         T Jr[3][3];
 #pragma unroll
-        for (int i = 0; i < 9; ++i) Jr[i / 3][i % 3] = r[(C_VAR + 1 + i) * NQ];
+        for (int i = 0; i < 9; ++i)
+          Jr[i / 3][i % 3] = a.ref_per_cell ? rec[(C_VAR + 1) * NQ + i] : r[(C_VAR + 1 + i) * NQ];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -786,6 +798,8 @@ KArgs<T> make_args(const lsmf_op *op) {
   a.cell_nodes = L.d_cell_nodes.ptr;
   a.n_cells = L.n_cells;
   a.ncomp = op->ncomp;
+  a.rec_elems = op->rec_elems;
+  a.ref_per_cell = op->ref_per_cell ? 1 : 0;
   a.table = (T *)op->d_table.ptr;
   a.src = nullptr;
   a.dst = nullptr;
@@ -841,7 +855,7 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
                         (LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD) &&
                     !(mask & MASK_INHOM);
   using SR = SFR<P, Q, T>;
-  const size_t rec_bytes = (size_t)op->ncomp * S::NQ * sizeof(T);
+  const size_t rec_bytes = (size_t)op->rec_elems * sizeof(T);
   const TabT<P, Q, T> tabt = make_tabt<P, Q, T>(op->mesh->basis);
   auto wbytes = [&](int st) { return ((st * rec_bytes + 8 * (st > 0 ? st : 1) + SR::SZ * sizeof(T) + 127) / 128) * 128; };
   // defaults measured on B200 (ring depth x warps per block swept for

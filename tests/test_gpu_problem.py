@@ -190,8 +190,8 @@ def test_adjoint_gradient_matches_oracle_gradient(formulation):
 
 def test_adjoint_config_size_finite_differences():
     """The adjoint benchmark workload (32^3 Q2 cube, 823,875 DoFs, log mu ~
-    N(0, 0.3^2), top-face misfit): 20 seeded directions at step 1e-6,
-    max |fd - g.v| <= 1e-6 max |fd|."""
+    N(0, 0.3^2), top-face misfit): 20 seeded +-1 directions (each cell's
+    log mu moves by the step 1e-6), max |fd - g.v| <= 1e-6 max |fd|."""
     import bench
     pb = lsmf.Problem(bench.adjoint_prm())
     assert pb.n_dofs == 823875

@@ -163,12 +163,15 @@ def test_bounded_wait_run_out_reports_timeout_and_recovers():
 def test_el_n_and_memory_consumption():
     gm, om, cmask, mu, u, src = _setup(p=2, coarse=(2, 2, 2), level=1)
     nc, nn, nd = gm.info()
-    for caching, ncomp in (("tensor4", 52), ("tensor2", 18), ("scalar", 20), ("tensor4_ns", 92)):
+    # values per cell record: ncomp per quadrature point; scalar caching on
+    # these affine cells keeps 11 per point and the reference inverse
+    # Jacobian once per cell (11 * 27 + 9 = 306)
+    for caching, rec in (("tensor4", 52 * 27), ("tensor2", 18 * 27), ("scalar", 306), ("tensor4_ns", 92 * 27)):
         op = lsmf.NeoHookOperator(gm, caching, 1, "fp64")
         assert op.m() == op.n() == nd
-        # cache tables (one record of ncomp values per quadrature point) plus
-        # the index map and the node coordinates; diagonals excluded
-        assert op.memory_consumption() == nc * ncomp * 27 * 8 + nc * 27 * 4 + nn * 3 * 8
+        # cache tables plus the index map and the node coordinates; diagonals
+        # excluded
+        assert op.memory_consumption() == nc * rec * 8 + nc * 27 * 4 + nn * 3 * 8
     op = lsmf.NeoHookOperator(gm, "tensor4", 1, "fp64")
     op.set_material(mu, 0.3)
     op.cache(torch.tensor(u, device="cuda"))
