@@ -203,6 +203,11 @@ lsmf_status lsmf_gmg_vmult(lsmf_gmg *g, double *d_dst, const double *d_src);
 lsmf_status lsmf_gmg_level_info(const lsmf_gmg *g, int level, double *out6);
 /* CUDA stream of every level operation (cudaStream_t) */
 lsmf_status lsmf_gmg_set_stream(lsmf_gmg *g, void *stream);
+/* the level operator of a level (the reference's mg_matrices[level],
+ * mf_elasticity.h:2046-2077), owned by the GMG object: for its options
+ * (lsmf_operator_set_option) and for inspection; a changed option takes
+ * effect from the next set-up */
+lsmf_status lsmf_gmg_level_operator(lsmf_gmg *g, int level, lsmf_op **op);
 /* options: LSMF_GMG_OPT_GRAPH = 1 (default) replays the V-cycle as one CUDA
  * graph (for a given pair of vmult buffers); the first vmult after a set-up
  * captures the new launch sequence and updates the executable graph in

@@ -484,6 +484,14 @@ lsmf_status lsmf_gmg_setup(lsmf_gmg *g, const double *d_u) {
   return g->desc.precision == LSMF_FP64 ? gmg_setup_impl<double>(g, d_u) : gmg_setup_impl<float>(g, d_u);
 }
 
+lsmf_status lsmf_gmg_level_operator(lsmf_gmg *g, int level, lsmf_op **op) {
+  if (!g || !op) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  if (level < 0 || level >= (int)g->levels.size()) { set_error("bad level"); return LSMF_ERR_INVALID_ARG; }
+  *op = g->levels[level].op;
+  g->vstale = true;  // options of the returned operator may change the captured V-cycle
+  return LSMF_OK;
+}
+
 lsmf_status lsmf_gmg_set_option(lsmf_gmg *g, int option, int value) {
   if (!g) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
   if (option == LSMF_GMG_OPT_GRAPH) {

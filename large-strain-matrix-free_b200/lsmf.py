@@ -96,6 +96,7 @@ SIGNATURES = {
     "lsmf_gmg_level_info": (ctypes.c_int, [vp, ctypes.c_int, dp]),
     "lsmf_gmg_set_stream": (ctypes.c_int, [vp, vp]),
     "lsmf_gmg_set_option": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+    "lsmf_gmg_level_operator": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(vp)]),
     "lsmf_cg_solve": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, vp, vp, vp, ctypes.c_double,
                                      ctypes.c_int, ctypes.POINTER(SolveInfo)]),
     "lsmf_problem_create": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(vp)]),
@@ -409,6 +410,13 @@ class GMG:
     def set_scatter(self, mode):
         """'atomic' (default) or 'colour8' for every level cell loop and transfer."""
         check(lib().lsmf_gmg_set_option(self.h, 2, SCATTER[mode] if isinstance(mode, str) else int(mode)))
+
+    def level_option(self, level, option, value):
+        """lsmf_operator_set_option on the operator of a level (effective
+        from the next set-up)."""
+        h = vp()
+        check(lib().lsmf_gmg_level_operator(self.h, level, ctypes.byref(h)))
+        check(lib().lsmf_operator_set_option(h, option, value))
 
     def level_info(self, level):
         out = np.zeros(6)

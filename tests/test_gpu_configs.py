@@ -73,7 +73,7 @@ def cube64():
 
 @pytest.mark.parametrize("caching,formulation", [("tensor4", 1), ("tensor2", 1), ("scalar", 1), ("scalar", 0),
                                                  ("scalar_referential", 1), ("tensor4_ns", 1)])
-def test_cube64_vmult_entrywise_vs_oracle(cube64, caching, formulation):
+def test_cube64_vmult_entrywise_vs_oracle(cube64, caching, formulation, parity):
     gm, om, cmask, mu, u, src = cube64
     ref = O.Operator(om, caching, formulation)
     ref.set_material(mu, 0.3)
@@ -91,6 +91,7 @@ def test_cube64_vmult_entrywise_vs_oracle(cube64, caching, formulation):
         op.vmult(ddst, dsrc)
         got = ddst.double().cpu().numpy()
         err = _rel(got, want)
+        parity("64^3 Q2 vmult %s f%d %s vs oracle FP64" % (caching, formulation, precision), err, tol)
         assert err < tol, (caching, precision, err)
         if precision == "fp64":
             assert np.array_equal(got[cmask == 1], src[cmask == 1])
@@ -106,7 +107,7 @@ def _void_mask():
     return O.void_mask(VOIDS["cells"], VOIDS["count"], VOIDS["radius"], VOIDS["seed"])
 
 
-def test_voids_mesh_and_operator_vs_oracle():
+def test_voids_mesh_and_operator_vs_oracle(parity):
     act = _void_mask()
     assert 0 < int((act == 0).sum()) < act.size
     gm = lsmf.Mesh("box", VOIDS["cells"], 1, degree=2, coarse_active=act)
@@ -139,7 +140,9 @@ def test_voids_mesh_and_operator_vs_oracle():
     dsrc = torch.tensor(src, device="cuda")
     ddst = torch.empty_like(dsrc)
     op.vmult(ddst, dsrc)
-    assert _rel(ddst.cpu().numpy(), ref.vmult(src)) < FP64_TOL
+    err = _rel(ddst.cpu().numpy(), ref.vmult(src))
+    parity("voids vmult tensor4 FP64", err, FP64_TOL)
+    assert err < FP64_TOL
     # one V-cycle, Chebyshev degree 4, FP64 and FP32 levels
     b = np.where(cmask == 1, 0.0, src)
     db = torch.tensor(b, device="cuda")
@@ -150,7 +153,9 @@ def test_voids_mesh_and_operator_vs_oracle():
         g.vmult(ddst, db)
         og = O.GMG(O.GEOM_BOX, VOIDS["cells"], 1, (0, 0, 0), (1, 1, 1), 1.0, 2, 3, "tensor4", 1,
                    precision == "fp32", mu, 0.3, spec, u, degree=4, coarse_active=act)
-        assert _rel(ddst.cpu().numpy(), og.vmult(b)) < tol, precision
+        err = _rel(ddst.cpu().numpy(), og.vmult(b))
+        parity("voids V-cycle %s levels" % precision, err, tol)
+        assert err < tol, precision
         for lev in range(2):
             gi, oi = g.level_info(lev), og.level_info(lev)
             assert gi[2] == oi[2]                            # Chebyshev degree
@@ -171,7 +176,7 @@ def _voids_prm(level_precision):
 
 
 @pytest.mark.parametrize("level_precision", ["float", "double"])
-def test_voids_newton_load_steps_vs_oracle(level_precision):
+def test_voids_newton_load_steps_vs_oracle(level_precision, parity):
     pb = lsmf.Problem(_voids_prm(level_precision))
     ref = O.newton(geometry=O.GEOM_BOX, coarse=VOIDS["cells"], n_refinements=1, caching="tensor4", formulation=1,
                    mu=1.0, nu=0.3, dirichlet=[(4, 7, (0, 0, 0)), (5, 4, (0, 0, -0.01))], end_time=0.2, dt=0.1,
@@ -183,6 +188,7 @@ def test_voids_newton_load_steps_vs_oracle(level_precision):
     res = pb.run()
     assert [s["newton_iterations"] for s in res["steps"]] == [s["newton_iterations"] for s in ref["steps"]]
     u = pb.solution()
+    parity("voids Newton, 2 load steps, %s levels: displacement" % level_precision, _rel(u, ref["u"]), U_TOL)
     assert _rel(u, ref["u"]) <= U_TOL
 
 
@@ -217,10 +223,11 @@ def test_cook_8x8x1_newton_counts_vs_oracle():
         assert np.max(np.abs(np.array(a["point_u"]) - b["point_u"])) <= 1e-6 * np.max(np.abs(b["point_u"]))
 
 
-def test_cook_8x8x1_tight_displacement_vs_oracle():
+def test_cook_8x8x1_tight_displacement_vs_oracle(parity):
     pb = lsmf.Problem(_cook_prm(dict(TIGHT, **{"Tolerance force": 1e-10})))
     res = pb.run()
     ref = _cook_oracle(**dict(TIGHT_ORACLE, tol_f=1e-10))
     assert ref["rc"] == 0
     assert [s["newton_iterations"] for s in res["steps"]] == [s["newton_iterations"] for s in ref["steps"]]
+    parity("Cook 8x8x1 x2 refinements, 5 load steps: displacement", _rel(pb.solution(), ref["u"]), U_TOL)
     assert _rel(pb.solution(), ref["u"]) <= U_TOL

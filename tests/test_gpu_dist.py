@@ -64,7 +64,7 @@ def _problem(n_parts, voids):
 
 @pytest.mark.parametrize("n_parts", [2, 3])
 @pytest.mark.parametrize("voids", [False, True])
-def test_group_vmult_dot_and_cg_equal_whole_mesh(n_parts, voids):
+def test_group_vmult_dot_and_cg_equal_whole_mesh(n_parts, voids, parity):
     gm, gop, gu, parts, rng = _problem(n_parts, voids)
     nd = gm.info()[2]
     D = lsmf.Dist.group([p["op"] for p in parts])
@@ -83,6 +83,8 @@ def test_group_vmult_dot_and_cg_equal_whole_mesh(n_parts, voids):
     torch.cuda.synchronize()
     for p, d in zip(parts, dsts):
         got = d.cpu().numpy()
+        parity("partitioned vmult, %d parts%s" % (n_parts, ", voids" if voids else ""),
+               np.max(np.abs(got[p["od"]] - want[p["gd"][p["od"]]])) / np.max(np.abs(want)), 1e-12)
         assert np.max(np.abs(got[p["od"]] - want[p["gd"][p["od"]]])) <= 1e-12 * np.max(np.abs(want))
         # ghost entries of the result are cleared
         ud = (3 * p["lay"]["upper_shared"][:, None] + np.arange(3)).reshape(-1)

@@ -39,7 +39,7 @@ def box():
 
 
 @pytest.mark.parametrize("caching,formulation", VARIANTS)
-def test_vmult_equals_assembled_tangent(box, caching, formulation):
+def test_vmult_equals_assembled_tangent(box, caching, formulation, parity):
     m, gm, cm, mu, u, K, rng = box
     x = rng.uniform(-1, 1, m.n_dofs)
     want = K[formulation] @ x
@@ -51,6 +51,8 @@ def test_vmult_equals_assembled_tangent(box, caching, formulation):
         out = torch.empty_like(dx)
         op.vmult(out, dx)
         got = out.double().cpu().numpy()
+        parity("vmult %s f%d %s vs assembled tangent" % (caching, formulation, precision),
+               np.max(np.abs(got - want)) / np.max(np.abs(want)), tol)
         assert np.max(np.abs(got - want)) <= tol * np.max(np.abs(want)), (caching, precision)
 
 

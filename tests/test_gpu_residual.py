@@ -44,7 +44,7 @@ def _box(formulation, scatter="atomic"):
 @pytest.mark.parametrize("geom", ["cook", "box"])
 @pytest.mark.parametrize("formulation", [0, 1])
 @pytest.mark.parametrize("scatter", ["atomic", "colour8"])
-def test_residual_matches_oracle(geom, formulation, scatter):
+def test_residual_matches_oracle(geom, formulation, scatter, parity):
     pb, om, dirichlet, neumann, t = (_cook if geom == "cook" else _box)(formulation, scatter)
     assert pb.n_dofs == om.n_dofs
     rng = np.random.default_rng(5)
@@ -58,6 +58,7 @@ def test_residual_matches_oracle(geom, formulation, scatter):
     dR = torch.full_like(du, 3.0)
     nrm = pb.residual(du, t, dR)
     R = dR.cpu().numpy()
+    parity("residual %s f%d %s" % (geom, formulation, scatter), np.max(np.abs(R - R_ref)) / np.max(np.abs(R_ref)), TOL)
     assert np.max(np.abs(R - R_ref)) <= TOL * np.max(np.abs(R_ref))
     assert abs(nrm - nrm_ref) <= TOL * nrm_ref
     assert np.all(R[cmask == 1] == 0.0)
