@@ -658,6 +658,25 @@ def run_lsmf(args):
                 "alg_GBps": round(by / (ms * 1e-3) / 1e9, 1), "frac_hbm": round(by / (ms * 1e-3) / 1e9 / peak, 3)}
             if v_op is not op:
                 del v_op
+    if not args.no_variants:
+        # the bit-reproducible scatter (8 colour launches, plain adds) beside
+        # the atomic default, tensor4 FP64
+        op.set_scatter("colour8")
+        d_out = torch.empty_like(src64)
+        for _ in range(2):
+            op.vmult(d_out, src64)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(5):
+            op.vmult(d_out, src64)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / 5
+        by = alg_bytes("tensor4", 8, n_nodes, n_qp, n_cells)
+        variants["tensor4_fp64_colour8"] = {
+            "gdofs": round(n_dofs / (ms * 1e-3) / 1e9, 3), "ms": round(ms, 4),
+            "alg_GBps": round(by / (ms * 1e-3) / 1e9, 1), "frac_hbm": round(by / (ms * 1e-3) / 1e9 / peak, 3)}
+        op.set_scatter("atomic")
 
     # end to end through the public API with host buffers: every step copies
     # its source from pinned host memory and its result back; the copies of

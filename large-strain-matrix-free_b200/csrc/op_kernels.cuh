@@ -867,6 +867,11 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
   // loads, as do tensor2 and scalar (latency / FP64 bound)
   const bool ring_variant = VAR == VAR_TENSOR4 || VAR == VAR_TENSOR4_NS || VAR == VAR_SCALAR_REF;
   int stages = op->stages >= 0 ? op->stages : ((ring_variant && rec_bytes <= 24 * 1024) ? 1 : 0);
+  // a level small enough that every warp gets at most one cell (a coarse
+  // multigrid level) gains nothing from the ring, which can only prefetch
+  // a warp's next cell: plain loads (15^3-cell FP64 coarse Chebyshev solve
+  // 10.9 -> 9.9 ms per V-cycle, FP32 unchanged)
+  if (op->stages < 0 && a.n_cells <= 32 * num_sms()) stages = 0;
   const int max_warps = op->max_warps > 0 ? op->max_warps : ((VAR == VAR_TENSOR2 && sizeof(T) == 8) ? 8 : 4);
   if (rec_bytes % 16 != 0) stages = 0;
   // fewer stages when the ring would leave fewer than 4 warps per block

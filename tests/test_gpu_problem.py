@@ -49,7 +49,10 @@ def test_cook_3d_golden_on_gpu(case):
             assert float("%g" % s["point_u"][c]) == gs["displacement"][c], (case, s, gs)
 
 
-TIGHT = {"Residual": 1e-13, "Tolerance force": 1e-11, "Tolerance displacement": 1e-10,
+# CG 1e-12 on the GPU: with FP32 levels the V-cycle varies by rounding from
+# one application to the next (atomic scatter), which erodes CG's
+# conjugacy near 1e-13; the decisions are made by the update norm either way
+TIGHT = {"Residual": 1e-12, "Tolerance force": 1e-11, "Tolerance displacement": 1e-10,
          "Max iterations Newton-Raphson": 25}
 TIGHT_ORACLE = dict(tol_lin=1e-13, tol_f=1e-11, tol_u=1e-10, max_nr=25)
 U_TOL = 1e-10
