@@ -240,6 +240,11 @@ lsmf_status lsmf_operator_set_option(lsmf_op *op, int option, int value) {
     op->wait_tries = value;
     return LSMF_OK;
   }
+  if (option == LSMF_OPT_RECORD_PREFETCH) {
+    if (value < 0 || value > 2) { set_error("record prefetch must be 0, 1 or 2"); return LSMF_ERR_INVALID_ARG; }
+    op->prefetch = value;
+    return LSMF_OK;
+  }
   if (option == LSMF_OPT_SCATTER) {
     if (value != LSMF_SCATTER_ATOMIC && value != LSMF_SCATTER_COLOUR8) {
       set_error("scatter must be 0 (atomic) or 1 (colour8)");

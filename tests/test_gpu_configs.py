@@ -17,8 +17,8 @@ oracle at each configuration's own size and mesh, through the C ABI.
   formulation 1, mu = 80.194, nu = 0.3, tensor4, GMG with FP32 levels, 5
   load steps: with the configuration's own tolerances (CG 1e-8, Newton 1e-9 /
   1e-6) the Newton iteration counts of every load step equal the oracle's;
-  solved tightly (CG 1e-12, Newton 1e-10 / 1e-10; the oracle CG 1e-13) the
-  displacement agrees within 1e-10 relative.
+  solved tightly (CG 1e-12, Newton 1e-10 / 1e-10) the displacement agrees
+  within 1e-10 relative.
 
 The tight Newton tolerances are set from the oracle's convergence history:
 the relative residual levels off (near 4e-13 on the small meshes, near 1e-11
@@ -49,7 +49,7 @@ FP64_TOL, FP32_TOL, U_TOL = 1e-10, 2e-5, 1e-10
 # conjugacy near 1e-13; the decisions are made by the update norm either way
 TIGHT = {"Residual": 1e-12, "Tolerance force": 1e-11, "Tolerance displacement": 1e-10,
          "Max iterations Newton-Raphson": 25}
-TIGHT_ORACLE = dict(tol_lin=1e-13, tol_f=1e-11, tol_u=1e-10, max_nr=25)
+TIGHT_ORACLE = dict(tol_lin=1e-12, tol_f=1e-11, tol_u=1e-10, max_nr=25)
 
 
 def _rel(a, b):

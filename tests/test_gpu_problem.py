@@ -54,7 +54,7 @@ def test_cook_3d_golden_on_gpu(case):
 # conjugacy near 1e-13; the decisions are made by the update norm either way
 TIGHT = {"Residual": 1e-12, "Tolerance force": 1e-11, "Tolerance displacement": 1e-10,
          "Max iterations Newton-Raphson": 25}
-TIGHT_ORACLE = dict(tol_lin=1e-13, tol_f=1e-11, tol_u=1e-10, max_nr=25)
+TIGHT_ORACLE = dict(tol_lin=1e-12, tol_f=1e-11, tol_u=1e-10, max_nr=25)
 U_TOL = 1e-10
 
 
