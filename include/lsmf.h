@@ -157,7 +157,8 @@ lsmf_status lsmf_operator_el(lsmf_op *op, int row, int col, double *value);
  *   (bit-reproducible vmult, for parity and debugging).
  * LSMF_OPT_RECORD_PREFETCH: with plain record loads, 1 issues an L1
  *   prefetch of the cell's record before its sum-factorisation sweeps, 2 of
- *   the next cell's record; 0 (default) none.
+ *   the next cell's record, 0 none; -1 (default): 1, except 0 for the FP64
+ *   scalar variant (measured).
  * A bounded device wait that runs out in the pipelined kernel is reported
  * as LSMF_ERR_TIMEOUT by lsmf_operator_sync, lsmf_cg_solve and the GMG
  * set-up (the next synchronising call on the operator). */
@@ -218,13 +219,8 @@ lsmf_status lsmf_gmg_level_operator(lsmf_gmg *g, int level, lsmf_op **op);
  * Chebyshev degree).  0 launches the kernels one by one.
  * LSMF_GMG_OPT_SCATTER: LSMF_SCATTER_ATOMIC (default) or
  * LSMF_SCATTER_COLOUR8 for every level operator, diagonal, restriction and
- * prolongation (a bit-reproducible V-cycle).
- * LSMF_GMG_OPT_FUSED_CHEBYSHEV: 1 (default) runs each Chebyshev step of a
- * level small enough that every warp gets at most one cell (the coarse
- * level) as one launch: the cell loop, after which the last cell to finish
- * around each block of nodes applies the step to those nodes; 0 keeps a
- * separate update kernel per step (atomic scatter only). */
-enum { LSMF_GMG_OPT_GRAPH = 1, LSMF_GMG_OPT_SCATTER = 2, LSMF_GMG_OPT_FUSED_CHEBYSHEV = 3 };
+ * prolongation (a bit-reproducible V-cycle). */
+enum { LSMF_GMG_OPT_GRAPH = 1, LSMF_GMG_OPT_SCATTER = 2 };
 lsmf_status lsmf_gmg_set_option(lsmf_gmg *g, int option, int value);
 
 /* ---- CG (SolverCG as driven by solve_linear_system, mf_elasticity.h:3012-3214) */

@@ -241,7 +241,7 @@ lsmf_status lsmf_operator_set_option(lsmf_op *op, int option, int value) {
     return LSMF_OK;
   }
   if (option == LSMF_OPT_RECORD_PREFETCH) {
-    if (value < 0 || value > 2) { set_error("record prefetch must be 0, 1 or 2"); return LSMF_ERR_INVALID_ARG; }
+    if (value < -1 || value > 2) { set_error("record prefetch must be -1 (auto), 0, 1 or 2"); return LSMF_ERR_INVALID_ARG; }
     op->prefetch = value;
     return LSMF_OK;
   }

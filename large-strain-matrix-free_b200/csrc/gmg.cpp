@@ -263,20 +263,6 @@ void chebyshev_coefficients(lsmf_cheb &c, int degree, double range) {
 // PreconditionChebyshev::vmult (zero_start) / step on the vectors x, b of
 // level l (the level's r and xold are the smoother's work vectors)
 template <typename T>
-lsmf_status chebyshev_run(lsmf_gmg *g, int l, T *x, const T *b, bool zero_start);
-
-int device_sms() {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
-  return sms;
-}
-
-template <typename T>
 lsmf_status chebyshev_run(lsmf_gmg *g, int l, T *x, const T *b, bool zero_start) {
   lsmf_gmg_level &GL = g->levels[l];
   lsmf_op *op = GL.op;
@@ -298,24 +284,12 @@ lsmf_status chebyshev_run(lsmf_gmg *g, int l, T *x, const T *b, bool zero_start)
   if (c.degree < 2 || std::fabs(c.delta) < 1e-40) return LSMF_OK;
   double rhok = c.delta / c.theta;
   const double sigma = c.theta / c.delta;
-  // a level where every warp gets at most one cell (the coarse level) runs
-  // each step as one launch: the cell loop with the update fused in; larger
-  // levels keep the cell loop and the vectorised update kernel
-  const bool fuse = g->fuse_cheb && op->scatter == LSMF_SCATTER_ATOMIC && op->L().n_cells <= 32 * device_sms();
   for (int k = 0; k < c.degree - 1; ++k) {
+    LSMF_TRY(launch_apply_cells(op, r, x));
     const double rhokp = 1. / (2. * sigma - rhok);
     const double f1 = rhokp * rhok, f2 = 2. * rhokp / c.delta;
     rhok = rhokp;
-    const bool has_old = !(zero_start && k == 0);
-    if (fuse) {
-      ChebStep cs;
-      cs.x = x; cs.xold = xold; cs.r = r; cs.b = b; cs.invd = invd; cs.cmask = cm;
-      cs.f1 = f1; cs.f2 = f2; cs.has_old = has_old;
-      LSMF_TRY(launch_apply_cells_cheb(op, cs));
-    } else {
-      LSMF_TRY(launch_apply_cells(op, r, x));
-      LSMF_TRY(cheb_step_async<T>(x, xold, b, r, invd, cm, f1, f2, has_old, n, st));
-    }
+    LSMF_TRY(cheb_step_async<T>(x, xold, b, r, invd, cm, f1, f2, !(zero_start && k == 0), n, st));
   }
   return LSMF_OK;
 }
@@ -522,11 +496,6 @@ lsmf_status lsmf_gmg_set_option(lsmf_gmg *g, int option, int value) {
   if (!g) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
   if (option == LSMF_GMG_OPT_GRAPH) {
     g->use_graph = value != 0;
-    drop_graph(g);
-    return LSMF_OK;
-  }
-  if (option == LSMF_GMG_OPT_FUSED_CHEBYSHEV) {
-    g->fuse_cheb = value != 0;
     drop_graph(g);
     return LSMF_OK;
   }

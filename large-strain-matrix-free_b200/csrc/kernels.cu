@@ -124,14 +124,6 @@ lsmf_status launch_apply_cells(const lsmf_op *op, void *dst, const void *src) {
   return for_cell_ranges(op->L(), op->scatter, [&](CellRange r) { return t->apply(op, dst, src, mask, r); });
 }
 
-// r += A_cells x and one Chebyshev step on x, xold, r, fused (ChebStep)
-lsmf_status launch_apply_cells_cheb(const lsmf_op *op, const ChebStep &cs) {
-  const OpsTable *t = table_of(op);
-  if (!t) return LSMF_ERR_UNSUPPORTED;
-  LSMF_TRY(build_cheb_map(op->L()));
-  return t->apply_cheb(op, cs);
-}
-
 // K g over the constrained columns: gather without zeroing, scatter skipping
 // constrained rows (dst zeroed first, no identity rows)
 lsmf_status launch_apply_inhomogeneous(const lsmf_op *op, void *dst, const void *g) {

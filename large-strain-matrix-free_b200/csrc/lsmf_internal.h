@@ -81,17 +81,6 @@ struct DevBuf {
   }
 };
 
-// Owner blocks of a level for the Chebyshev step fused into the cell loop:
-// every node is owned by the first cell (in cell order) that contains it; a
-// cell's block is the set of nodes it owns.  contrib lists, per cell, the
-// blocks whose nodes that cell touches; need counts, per block, the cells
-// touching its nodes; count holds the arrivals of the running launch (zero
-// between launches).
-struct ChebFuseMap {
-  bool built = false;
-  DevBuf<int> own_off, own_nodes, contrib_off, contrib, need, count;
-};
-
 // One level of the structured hierarchy.
 struct Level {
   int p = 2, q = 3;
@@ -111,7 +100,6 @@ struct Level {
   std::vector<int> colour_cells;
   int colour_off[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   DevBuf<int> d_colour_cells;
-  ChebFuseMap cheb_map;
   // device
   DevBuf<int> d_cell_nodes;     // packed with constraint bits
   DevBuf<double> d_X;
@@ -188,7 +176,7 @@ struct lsmf_op {
   bool basic = false;                // use the basic (smem-sweep) vmult kernel
   int max_warps = 0;                 // warps per block cap of the vmult kernel (<= 8, 0 auto)
   int wait_tries = -1;               // bulk-copy wait bound (try_wait calls; -1 = default 2^22)
-  int prefetch = 0;                  // plain-load kernels: L1 prefetch of the record (0, 1 this cell, 2 next)
+  int prefetch = -1;                 // plain-load kernels: L1 prefetch of the record (0, 1 this cell, 2 next; -1 auto)
   int device = 0;                    // CUDA device the operator's buffers live on
   int scatter = LSMF_SCATTER_ATOMIC; // cell-loop scatter: atomics or the 8 colour launches
   cudaStream_t stream = 0;
@@ -206,8 +194,6 @@ lsmf_status launch_apply(const lsmf_op *op, void *dst, const void *src, unsigned
 // identity rows); callers fold those into their own element-wise kernels
 lsmf_status launch_apply_cells(const lsmf_op *op, void *dst, const void *src);
 lsmf_status launch_diagonal(lsmf_op *op);
-// the level's owner blocks for the fused Chebyshev step (built once)
-lsmf_status build_cheb_map(Level &L);
 lsmf_status upload_basis_tables(const Basis &b);
 int table_components(int caching, int formulation, lsmf_precision precision);
 }  // namespace lsmf

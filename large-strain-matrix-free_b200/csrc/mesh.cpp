@@ -292,50 +292,6 @@ static lsmf_status build_transfer(const lsmf_mesh &M, const Level &C, const Leve
   return LSMF_OK;
 }
 
-// Owner blocks of the fused Chebyshev step (ChebFuseMap): node -> first cell
-// containing it; per cell the distinct blocks its nodes belong to (at most
-// the 27 cells around it, so at most 27 entries: one per lane of a warp);
-// per block the number of cells touching its nodes.
-lsmf_status build_cheb_map(Level &L) {
-  ChebFuseMap &M = L.cheb_map;
-  if (M.built) return LSMF_OK;
-  const int ncn = L.ncn();
-  std::vector<int> owner(L.n_nodes, -1);
-  for (int c = 0; c < L.n_cells; ++c)
-    for (int a = 0; a < ncn; ++a) {
-      const int n = L.cell_nodes[(size_t)c * ncn + a];
-      if (owner[n] < 0) owner[n] = c;
-    }
-  std::vector<int> own_off(L.n_cells + 1, 0), own_nodes(L.n_nodes);
-  for (int n = 0; n < L.n_nodes; ++n) own_off[owner[n] + 1]++;
-  for (int c = 0; c < L.n_cells; ++c) own_off[c + 1] += own_off[c];
-  {
-    std::vector<int> fill(own_off.begin(), own_off.end() - 1);
-    for (int n = 0; n < L.n_nodes; ++n) own_nodes[fill[owner[n]]++] = n;
-  }
-  std::vector<int> contrib_off(L.n_cells + 1, 0), contrib, need(L.n_cells, 0);
-  std::vector<int> blocks;
-  for (int c = 0; c < L.n_cells; ++c) {
-    blocks.clear();
-    for (int a = 0; a < ncn; ++a) {
-      const int o = owner[L.cell_nodes[(size_t)c * ncn + a]];
-      if (std::find(blocks.begin(), blocks.end(), o) == blocks.end()) blocks.push_back(o);
-    }
-    if (blocks.size() > 32) { set_error("owner-block list longer than a warp"); return LSMF_ERR_UNSUPPORTED; }
-    for (int o : blocks) { contrib.push_back(o); need[o]++; }
-    contrib_off[c + 1] = (int)contrib.size();
-  }
-  LSMF_TRY(M.own_off.upload(own_off.data(), own_off.size()));
-  LSMF_TRY(M.own_nodes.upload(own_nodes.data(), own_nodes.size()));
-  LSMF_TRY(M.contrib_off.upload(contrib_off.data(), contrib_off.size()));
-  LSMF_TRY(M.contrib.upload(contrib.data(), contrib.size()));
-  LSMF_TRY(M.need.upload(need.data(), need.size()));
-  LSMF_TRY(M.count.alloc(L.n_cells));
-  LSMF_CUDA(cudaMemset(M.count.ptr, 0, (size_t)L.n_cells * sizeof(int)));
-  M.built = true;
-  return LSMF_OK;
-}
-
 // Global node numbers and interface lists of a z-slab part on the finest
 // level L (see PartLayout).  A lattice point is a node of the whole mesh when
 // an active cell touches it; the whole mesh numbers its nodes in lattice

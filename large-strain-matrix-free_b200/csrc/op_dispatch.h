@@ -16,27 +16,12 @@ struct CellRange {
   bool plain = false;
 };
 
-// One Chebyshev step applied by the last contributor of each owner block
-// (see ChebFuseMap): x_new = x + f1 (x - xold) + f2 D^-1 (b - A x), xold = x,
-// r = 0, where A x is the cell contributions accumulated in r plus the
-// identity rows of the constrained dofs.
-struct ChebStep {
-  void *x, *xold, *r;
-  const void *b, *invd;
-  const uint8_t *cmask;
-  double f1, f2;
-  bool has_old;
-};
-
 struct OpsTable {
   lsmf_status (*cache)(lsmf_op *op);
   // cell loop only: dst += sum of the cell contributions (MFMask stages in
   // `mask`, internal bit MASK_INHOM_BIT: gather constrained entries)
   lsmf_status (*apply)(const lsmf_op *op, void *dst, const void *src, unsigned mask, CellRange range);
   lsmf_status (*diag)(lsmf_op *op, void *diag, CellRange range);
-  // cell loop r += A_cells x with the Chebyshev step fused (plain loads,
-  // atomic scatter; the level's ChebFuseMap must be built)
-  lsmf_status (*apply_cheb)(const lsmf_op *op, const ChebStep &cs);
 };
 
 // gather constrained entries instead of zeroing them (the inhomogeneity

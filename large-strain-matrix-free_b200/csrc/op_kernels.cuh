@@ -43,14 +43,6 @@ struct KArgs {
   int prefetch;          // plain loads: L1 prefetch of the record (0 off, 1 this cell, 2 the next cell)
   const int *cells;      // cell list of one colour (nullptr: all n_cells cells)
   int plain;             // scatter with plain adds (colour launches) instead of atomics
-  // fused Chebyshev step (apply_fast_kernel with CHEB): x is src, r is dst
-  T *cx, *cxold;
-  const T *cb, *cinvd;
-  const uint8_t *ccm;
-  double cf1, cf2;
-  int chas_old;
-  const int *own_off, *own_nodes, *contrib_off, *contrib, *need;
-  int *count;
 };
 
 // cell of list entry i
@@ -408,12 +400,7 @@ __global__ void __launch_bounds__(256) apply_kernel(KArgs<T> a, Tab<P, Q> tab) {
 // loop runs over the cell list of one lattice colour (a.cells, a.n_cells
 // entries) and scatters with plain adds; otherwise over all cells with
 // atomics.
-// CHEB: after its scatter, the warp announces its cell to the owner blocks
-// its nodes touch; the warp whose arrival completes a block applies one
-// Chebyshev step to that block's nodes (every cell touching them has
-// scattered and, before that, gathered x, so nothing reads those x values
-// later in the launch).  No warp waits for another.
-template <int P, int Q, typename T, int VAR, int STAGES, bool COL, bool CHEB = false>
+template <int P, int Q, typename T, int VAR, int STAGES, bool COL>
 __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, T> tab) {
   constexpr bool SCALAR = (VAR == VAR_SCALAR_F0 || VAR == VAR_SCALAR_F1);
   // branch-free sweeps and point loop for the scalar variants (48^3 / 64^3
@@ -635,37 +622,6 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
         }
       }
     }
-    if (CHEB) {
-      // release: this lane's contributions are visible before the arrival
-      __threadfence();
-      __syncwarp();
-      const int c = cid(cell);
-      const int b0 = __ldg(a.contrib_off + c), nb = __ldg(a.contrib_off + c + 1) - b0;
-      int ob = -1, last = 0;
-      if (lane < nb) {
-        ob = __ldg(a.contrib + b0 + lane);
-        last = atomicAdd(a.count + ob, 1) == __ldg(a.need + ob) - 1;
-      }
-      unsigned todo = __ballot_sync(0xffffffffu, last);
-      while (todo) {
-        const int src = __ffs(todo) - 1;
-        todo &= todo - 1;
-        const int blk = __shfl_sync(0xffffffffu, ob, src);
-        __threadfence();  // acquire: every contribution to the block's nodes
-        const int n0 = __ldg(a.own_off + blk), nn = __ldg(a.own_off + blk + 1) - n0;
-        for (int e = lane; e < 3 * nn; e += 32) {
-          const size_t dof = 3 * (size_t)__ldg(a.own_nodes + n0 + e / 3) + e % 3;
-          const double xi = (double)__ldcg(a.cx + dof);
-          const double ax = (double)__ldcg(a.dst + dof) + (a.ccm[dof] ? xi : 0.0);
-          const double xo = a.chas_old ? (double)a.cxold[dof] : 0.0;
-          const double xn = xi + a.cf1 * (xi - xo) + a.cf2 * (double)a.cinvd[dof] * ((double)a.cb[dof] - ax);
-          a.cxold[dof] = T(xi);
-          a.cx[dof] = T(xn);
-          a.dst[dof] = T(0);
-        }
-        if (lane == 0) a.count[blk] = 0;  // ready for the next launch
-      }
-    }
   }
 }
 
@@ -869,13 +825,6 @@ KArgs<T> make_args(const lsmf_op *op) {
   a.cells = nullptr;
   a.plain = 0;
   a.prefetch = op->prefetch;
-  a.cx = a.cxold = nullptr;
-  a.cb = a.cinvd = nullptr;
-  a.ccm = nullptr;
-  a.cf1 = a.cf2 = 0;
-  a.chas_old = 0;
-  a.own_off = a.own_nodes = a.contrib_off = a.contrib = a.need = nullptr;
-  a.count = nullptr;
   return a;
 }
 
@@ -911,6 +860,11 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
   a.mask = mask;
   set_range(a, range);
   if (a.n_cells == 0) return LSMF_OK;
+  // L1 prefetch of each cell's record before its sweeps (plain-load
+  // kernels): measured on B200 at 64^3 Q2 and 48^3 Q4 it shortens every
+  // plain-load kernel (Q4 tensor4 FP64 1.37 -> 1.19 ms, Q2 tensor2 FP32
+  // -6 %) except the FP64 scalar variant (+1 %), which keeps it off
+  if (op->prefetch < 0) a.prefetch = ((VAR == VAR_SCALAR_F0 || VAR == VAR_SCALAR_F1) && sizeof(T) == 8) ? 0 : 1;
   const Tab<P, Q> tab = make_tab<P, Q>(op->mesh->basis);
   using S = SF<P, Q, T>;
   const int w = warps_for(sizeof(T) * S::SZ, 8);
@@ -982,40 +936,6 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
 }
 
 template <int P, int Q, typename T, int VAR>
-lsmf_status run_apply_cheb(const lsmf_op *op, const ChebStep &cs) {
-  const ChebFuseMap &M = op->L().cheb_map;
-  if (!M.built) { set_error("the level's owner blocks are not built"); return LSMF_ERR_NOT_INITIALIZED; }
-  auto a = make_args<T>(op);
-  a.src = (const T *)cs.x;
-  a.dst = (T *)cs.r;
-  a.cx = (T *)cs.x;
-  a.cxold = (T *)cs.xold;
-  a.cb = (const T *)cs.b;
-  a.cinvd = (const T *)cs.invd;
-  a.ccm = cs.cmask;
-  a.cf1 = cs.f1;
-  a.cf2 = cs.f2;
-  a.chas_old = cs.has_old ? 1 : 0;
-  a.own_off = M.own_off.ptr;
-  a.own_nodes = M.own_nodes.ptr;
-  a.contrib_off = M.contrib_off.ptr;
-  a.contrib = M.contrib.ptr;
-  a.need = M.need.ptr;
-  a.count = M.count.ptr;
-  using SR = SFR<P, Q, T>;
-  const TabT<P, Q, T> tabt = make_tabt<P, Q, T>(op->mesh->basis);
-  const size_t wb = ((8 + SR::SZ * sizeof(T) + 127) / 128) * 128;  // plain loads: no ring
-  const int w = warps_for_budget(wb, op->max_warps > 0 ? op->max_warps : 4, 220 * 1024);
-  const size_t smem = w * wb;
-  auto k = apply_fast_kernel<P, Q, T, VAR, 0, false, true>;
-  LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int g = grid_for(k, 32 * w, smem, (a.n_cells + w - 1) / w);
-  k<<<g, 32 * w, smem, op->stream>>>(a, tabt);
-  LSMF_CUDA(cudaGetLastError());
-  return LSMF_OK;
-}
-
-template <int P, int Q, typename T, int VAR>
 lsmf_status run_diag(lsmf_op *op, T *diag, CellRange range) {
   auto a = make_args<T>(op);
   a.dst = diag;
@@ -1058,11 +978,8 @@ struct DegreeOps {
   static lsmf_status diag(lsmf_op *op, void *d, CellRange range) {
     return LSMF_DISPATCH_VAR(variant_of(op), (run_diag<P, Q, T, V_>(op, (T *)d, range)));
   }
-  static lsmf_status apply_cheb(const lsmf_op *op, const ChebStep &cs) {
-    return LSMF_DISPATCH_VAR(variant_of(op), (run_apply_cheb<P, Q, T, V_>(op, cs)));
-  }
   static const OpsTable &table() {
-    static const OpsTable t = {&cache, &apply, &diag, &apply_cheb};
+    static const OpsTable t = {&cache, &apply, &diag};
     return t;
   }
 };

@@ -5,13 +5,8 @@
 #include <vector>
 
 #include "lsmf_internal.h"
-#include "op_dispatch.h"
 
 namespace lsmf {
-
-// r += A_cells x with one Chebyshev step fused into the cell loop (the last
-// contributor of each owner block updates it; kernels.cu)
-lsmf_status launch_apply_cells_cheb(const lsmf_op *op, const ChebStep &cs);
 
 // device scalar slots used by the CG kernels
 enum { SC_DH = 0, SC_RES2 = 1, SC_GH0 = 2, SC_GH1 = 3, SC_TMP = 4, SC_N = 8 };
@@ -126,7 +121,6 @@ struct lsmf_gmg {
   // launch sequence is unchanged
   bool use_graph = true;
   int scatter = LSMF_SCATTER_ATOMIC;  // cell loops and transfers: atomics or colour8
-  bool fuse_cheb = true;              // small levels: Chebyshev step fused into the cell loop
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t vexec = nullptr;
   bool vstale = true;

@@ -411,10 +411,6 @@ class GMG:
         """'atomic' (default) or 'colour8' for every level cell loop and transfer."""
         check(lib().lsmf_gmg_set_option(self.h, 2, SCATTER[mode] if isinstance(mode, str) else int(mode)))
 
-    def set_fused_chebyshev(self, enable):
-        """Fuse each Chebyshev step into the cell loop on levels where every
-        warp gets at most one cell (default on)."""
-        check(lib().lsmf_gmg_set_option(self.h, 3, int(bool(enable))))
 
     def level_option(self, level, option, value):
         """lsmf_operator_set_option on the operator of a level (effective

@@ -190,32 +190,3 @@ def test_vcycle_coarse_cg_matches_oracle(precision):
     tol = 1e-9 if precision == "fp64" else 1e-4
     assert np.max(np.abs(ddst.cpu().numpy() - want)) <= tol * np.max(np.abs(want))
 
-
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_fused_chebyshev_step_equals_separate_update(precision):
-    """On levels where every warp gets at most one cell, each Chebyshev step
-    runs as one launch: the cell loop, then the last cell around each block
-    of nodes applies the update to it.  The V-cycle equals the one with a
-    separate update kernel per step (the two differ only in the order of
-    the floating-point atomics), and both equal the oracle's."""
-    gm, mu, u, dirichlet, (lo, hi), rng = _problem("tensor4", 1)
-    src = rng.uniform(-1, 1, u.size)
-    src[gm.constraint_mask() == 1] = 0
-    dsrc = torch.tensor(src, device="cuda")
-    du = torch.tensor(u, device="cuda")
-    out = {}
-    for fused in (True, False):
-        g = lsmf.GMG(gm, "tensor4", 1, precision)
-        g.set_fused_chebyshev(fused)
-        g.set_material(mu, 0.3)
-        g.setup(du)
-        d = torch.empty_like(dsrc)
-        for _ in range(2):                    # the second V-cycle reuses the counters
-            g.vmult(d, dsrc)
-        out[fused] = d.cpu().numpy()
-    tol = 1e-12 if precision == "fp64" else 1e-5
-    assert np.max(np.abs(out[True] - out[False])) <= tol * np.max(np.abs(out[False]))
-    og = O.GMG(O.GEOM_BOX, (1, 1, 1), 2, lo, hi, 1.0, 2, 3, "tensor4", 1, precision == "fp32", mu, 0.3,
-               dirichlet, u)
-    want = og.vmult(src)
-    assert np.max(np.abs(out[True] - want)) <= (1e-10 if precision == "fp64" else 1e-4) * np.max(np.abs(want))
