@@ -361,12 +361,14 @@ def adjoint_prm(cells=8, refinements=2, formulation=1, level_precision="float", 
     residual 1e-11 and update 1e-10, no absolute stop: the relative residual
     levels off near 1e-13 while the update keeps falling, so both tests pass
     with a wide margin) with GMG levels of the given precision and an FP64
-    outer CG to 1e-13."""
+    outer CG to 1e-10 of the current residual (the last Newton iteration
+    starts near the residual's rounding floor, which a stricter CG cannot
+    always reduce further)."""
     keys = [("Finite element system", [("Polynomial degree", 2), ("Quadrature order", 3)]),
             ("Geometry", [("Dimension", 3), ("Type", "Box"), ("Box cells", "%d, %d, %d" % ((cells,) * 3)),
                           ("Global refinement", refinements)]),
             ("Material properties", [("Shear modulus", 1.0), ("Poisson's ratio", 0.3), ("Formulation", formulation)]),
-            ("Linear solver", [("Solver type", "MF_CG"), ("Residual", 1e-13), ("Preconditioner type", "gmg"),
+            ("Linear solver", [("Solver type", "MF_CG"), ("Residual", 1e-10), ("Preconditioner type", "gmg"),
                                ("MF caching", "tensor4" if formulation == 1 else "scalar"),
                                ("MF level precision", level_precision), ("MF scatter", scatter)]),
             ("Nonlinear solver", [("Max iterations Newton-Raphson", 25), ("Tolerance force", 1e-11),

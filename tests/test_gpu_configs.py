@@ -17,7 +17,7 @@ oracle at each configuration's own size and mesh, through the C ABI.
   formulation 1, mu = 80.194, nu = 0.3, tensor4, GMG with FP32 levels, 5
   load steps: with the configuration's own tolerances (CG 1e-8, Newton 1e-9 /
   1e-6) the Newton iteration counts of every load step equal the oracle's;
-  solved tightly (CG 1e-12, Newton 1e-10 / 1e-10) the displacement agrees
+  solved tightly (CG 1e-10, Newton 1e-10 / 1e-10) the displacement agrees
   within 1e-10 relative.
 
 The tight Newton tolerances are set from the oracle's convergence history:
@@ -44,12 +44,14 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 import bench  # noqa: E402
 
 FP64_TOL, FP32_TOL, U_TOL = 1e-10, 2e-5, 1e-10
-# CG 1e-12 on the GPU: with FP32 levels the V-cycle varies by rounding from
-# one application to the next (atomic scatter), which erodes CG's
-# conjugacy near 1e-13; the decisions are made by the update norm either way
-TIGHT = {"Residual": 1e-12, "Tolerance force": 1e-11, "Tolerance displacement": 1e-10,
+# CG 1e-10 relative to the current residual: the last Newton iteration
+# starts from a residual near its rounding floor, and a CG asked to reduce
+# that by 1e-12 or more can stall when the V-cycle varies by rounding from
+# one application to the next (atomic scatter); the convergence decisions
+# are made by the update norm with wide margins either way
+TIGHT = {"Residual": 1e-10, "Tolerance force": 1e-11, "Tolerance displacement": 1e-10,
          "Max iterations Newton-Raphson": 25}
-TIGHT_ORACLE = dict(tol_lin=1e-12, tol_f=1e-11, tol_u=1e-10, max_nr=25)
+TIGHT_ORACLE = dict(tol_lin=1e-10, tol_f=1e-11, tol_u=1e-10, max_nr=25)
 
 
 def _rel(a, b):

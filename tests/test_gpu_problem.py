@@ -4,7 +4,7 @@
    formulation 0, scalar caching, Jacobi-CG) through lsmf_problem: mesh size,
    volume, Newton iterations and the printed displacement to 6 digits.
 2. GMG-CG Newton (FP32 and FP64 levels) against the CPU oracle's Newton,
-   both solved tightly (CG 1e-13, Newton force 1e-11 / displacement 1e-10
+   both solved tightly (CG 1e-10, Newton force 1e-11 / displacement 1e-10
    relative; the relative residual levels off near 4e-13 while the update
    keeps falling, so each convergence decision has a wide margin):
    identical Newton iteration counts, displacement within 1e-10 relative.
@@ -49,12 +49,14 @@ def test_cook_3d_golden_on_gpu(case):
             assert float("%g" % s["point_u"][c]) == gs["displacement"][c], (case, s, gs)
 
 
-# CG 1e-12 on the GPU: with FP32 levels the V-cycle varies by rounding from
-# one application to the next (atomic scatter), which erodes CG's
-# conjugacy near 1e-13; the decisions are made by the update norm either way
-TIGHT = {"Residual": 1e-12, "Tolerance force": 1e-11, "Tolerance displacement": 1e-10,
+# CG 1e-10 relative to the current residual: the last Newton iteration
+# starts from a residual near its rounding floor, and a CG asked to reduce
+# that by 1e-12 or more can stall when the V-cycle varies by rounding from
+# one application to the next (atomic scatter); the convergence decisions
+# are made by the update norm with wide margins either way
+TIGHT = {"Residual": 1e-10, "Tolerance force": 1e-11, "Tolerance displacement": 1e-10,
          "Max iterations Newton-Raphson": 25}
-TIGHT_ORACLE = dict(tol_lin=1e-12, tol_f=1e-11, tol_u=1e-10, max_nr=25)
+TIGHT_ORACLE = dict(tol_lin=1e-10, tol_f=1e-11, tol_u=1e-10, max_nr=25)
 U_TOL = 1e-10
 
 
@@ -189,7 +191,7 @@ def test_adjoint_gradient_matches_oracle_gradient(formulation, parity):
                                  caching="tensor4" if formulation == 1 else "scalar", formulation=formulation,
                                  mu=1.0, nu=0.3, dirichlet=[(4, 7, (0, 0, 0))],
                                  neumann=[(5, (0, 0, 0), (0.02, 0, -0.05))], end_time=1.0, dt=1.0,
-                                 tol_lin=1e-13, tol_f=1e-11, tol_u=1e-10, max_nr=25, precond="gmg",
+                                 tol_lin=1e-10, tol_f=1e-11, tol_u=1e-10, max_nr=25, precond="gmg",
                                  level_fp32=False)
     assert abs(J - Jref) <= 1e-10 * Jref
     assert np.max(np.abs(pb.solution() - uref)) <= 1e-10 * np.max(np.abs(uref))
