@@ -9,6 +9,7 @@
 // scalar (the residual norm) per CG iteration.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <limits>
 #include <new>
@@ -654,7 +655,14 @@ lsmf_status lsmf_cg_solve(lsmf_op *A, int precond, double omega, lsmf_gmg *gmg, 
     set_error("a bounded device wait timed out in the vmult kernel");
     return LSMF_ERR_TIMEOUT;
   }
-  if (!conv) { set_error("CG did not reach the tolerance"); return LSMF_ERR_CG_NOT_CONVERGED; }
+  if (!conv) {
+    // the facts of deal.II's SolverControl::NoConvergence: last step and value
+    char msg[160];
+    std::snprintf(msg, sizeof msg, "CG did not reach the tolerance (|g| = %.3e after %d iterations, tolerance %.3e)",
+                  res, it, tol_abs);
+    set_error(msg);
+    return LSMF_ERR_CG_NOT_CONVERGED;
+  }
   return LSMF_OK;
 }
 

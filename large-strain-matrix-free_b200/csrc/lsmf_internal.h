@@ -9,7 +9,9 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/lsmf.h"
@@ -44,6 +46,14 @@ struct Basis {
   void eval(double x, double *val, double *der) const;
 };
 
+// LSMF_POISON_ALLOC set (any value) in the environment: every new device
+// buffer of floating-point values (and the byte buffers that hold them:
+// records, level vectors, diagonals) is filled with 0xFF bytes, a NaN in
+// FP32 and FP64, so that a value read before it is written shows up as a
+// NaN instead of whatever the allocator hands back.  Index and mask buffers
+// are left alone.  Read at every allocation, so a process can switch it.
+inline bool poison_alloc() { return std::getenv("LSMF_POISON_ALLOC") != nullptr; }
+
 template <typename T>
 struct DevBuf {
   T *ptr = nullptr;
@@ -72,6 +82,13 @@ struct DevBuf {
       return LSMF_ERR_ALLOC;
     }
     n = count;
+    if constexpr (std::is_floating_point<T>::value || std::is_same<T, char>::value) {
+      if (poison_alloc()) {
+        e = cudaMemset(ptr, 0xFF, count * sizeof(T));
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();  // ordered before every stream's work
+        if (e != cudaSuccess) { set_error(std::string("cudaMemset: ") + cudaGetErrorString(e)); return LSMF_ERR_CUDA; }
+      }
+    }
     return LSMF_OK;
   }
   lsmf_status upload(const T *h, size_t count) {

@@ -76,9 +76,11 @@ __global__ void cg_update_kernel(double *x, double *g, const double *d, const do
 // CG direction: beta = sc[gh_new] / sc[gh_old]; d = beta d - h (beta = 0: d = -h)
 __global__ void cg_dir_kernel(double *d, const double *h, size_t n, const double *sc, int gh_new, int gh_old,
                               int first) {
+  // the first direction does not read d: it holds whatever the allocation
+  // held (0 * NaN would be NaN)
   const double beta = first ? 0.0 : sc[gh_new] / sc[gh_old];
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    d[i] = beta * d[i] - h[i];
+    d[i] = first ? -h[i] : beta * d[i] - h[i];
 }
 
 // 16-byte vectors of level values (4 floats / 2 doubles) for the
