@@ -159,11 +159,18 @@ lsmf_status lsmf_operator_el(lsmf_op *op, int row, int col, double *value);
  *   prefetch of the cell's record before its sum-factorisation sweeps, 2 of
  *   the next cell's record, 0 none; -1 (default): 1, except 0 for the FP64
  *   scalar variant (measured).
+ * LSMF_OPT_CELL_PAIRS: FP32 operators only: 1 = the vmult cell loop takes
+ *   two cells per warp and runs their sum factorisation and point physics
+ *   as the two halves of packed FP32x2 registers (one sm_100 f32x2
+ *   instruction for both cells); 0 = one cell per warp; -1 (default) =
+ *   measured choice (pairs for Q1 tensor2 / scalar formulation 1, Q2
+ *   tensor2 / scalar formulation 1 / scalar_referential, Q4
+ *   scalar_referential).  Ignored for FP64 operators.
  * A bounded device wait that runs out in the pipelined kernel is reported
  * as LSMF_ERR_TIMEOUT by lsmf_operator_sync, lsmf_cg_solve and the GMG
  * set-up (the next synchronising call on the operator). */
 enum { LSMF_OPT_BULK_PIPELINE = 1, LSMF_OPT_BASIC_KERNEL = 2, LSMF_OPT_MAX_WARPS = 3, LSMF_OPT_WAIT_TRIES = 4,
-       LSMF_OPT_SCATTER = 5, LSMF_OPT_RECORD_PREFETCH = 6 };
+       LSMF_OPT_SCATTER = 5, LSMF_OPT_RECORD_PREFETCH = 6, LSMF_OPT_CELL_PAIRS = 7 };
 enum { LSMF_SCATTER_ATOMIC = 0, LSMF_SCATTER_COLOUR8 = 1 };
 lsmf_status lsmf_operator_set_option(lsmf_op *op, int option, int value);
 /* Wait for the operator's stream and report a device error its kernels

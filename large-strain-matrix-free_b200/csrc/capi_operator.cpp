@@ -245,6 +245,11 @@ lsmf_status lsmf_operator_set_option(lsmf_op *op, int option, int value) {
     op->prefetch = value;
     return LSMF_OK;
   }
+  if (option == LSMF_OPT_CELL_PAIRS) {
+    if (value < -1 || value > 1) { set_error("cell pairs must be -1 (auto), 0 or 1"); return LSMF_ERR_INVALID_ARG; }
+    op->pairs = value;
+    return LSMF_OK;
+  }
   if (option == LSMF_OPT_SCATTER) {
     if (value != LSMF_SCATTER_ATOMIC && value != LSMF_SCATTER_COLOUR8) {
       set_error("scatter must be 0 (atomic) or 1 (colour8)");
@@ -303,6 +308,12 @@ lsmf_status lsmf_operator_sync(lsmf_op *op) {
     LSMF_CUDA(cudaStreamSynchronize(op->stream));
     set_error("a bounded device wait timed out in the vmult kernel; the result of that vmult is incomplete");
     return LSMF_ERR_TIMEOUT;
+  }
+  if (flag & 4) {
+    LSMF_CUDA(cudaMemsetAsync(op->d_flag.ptr, 0, sizeof(int), op->stream));
+    LSMF_CUDA(cudaStreamSynchronize(op->stream));
+    set_error("a vmult kernel was launched with less shared memory than its layout needs and did no work");
+    return LSMF_ERR_CUDA;
   }
   return LSMF_OK;
 }

@@ -50,15 +50,15 @@ struct TabT {
 // points of the cell record (collocation derivative, the
 // FEEvaluationImplCollocation step of mf_nh_operator.h:1271-1300) and the
 // reference inverse Jacobian
-template <int Q, typename T, typename DC>
-__device__ __forceinline__ void collocation_F(const T *__restrict__ rec, int q, const DC &Dc, const T Ji[3][3],
-                                              T F[3][3]) {
+// (R: the record, a pointer or an accessor with operator[] and + offset)
+template <int Q, typename T, typename DC, typename R>
+__device__ __forceinline__ void collocation_F(const R &rec, int q, const DC &Dc, const T Ji[3][3], T F[3][3]) {
   constexpr int NQ = Q * Q * Q;
   const int qx = q % Q, qy = (q / Q) % Q, qz = q / (Q * Q);
   T G[3][3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const T *u = rec + (C_VAR + 1 + c) * NQ;
+    const auto u = rec + (C_VAR + 1 + c) * NQ;
     T gx = 0, gy = 0, gz = 0;
 #pragma unroll
     for (int m = 0; m < Q; ++m) {
@@ -570,9 +570,10 @@ struct ScalarState {
 };
 
 // Q(g) of do_operation_on_cell (mf_nh_operator.h:922-1499) for the point
-// whose record is rec[comp * NQ] (rec already offset by q).
-template <typename T, int VAR, int NQ>
-__device__ __forceinline__ void physics(const T g[3][3], const T *__restrict__ rec, T mu, T lambda, T kappa,
+// whose record is rec[comp * NQ] (rec already offset by q; a pointer, or an
+// accessor with operator[] such as the record pair of two cells).
+template <typename T, int VAR, int NQ, typename R>
+__device__ __forceinline__ void physics(const T g[3][3], const R &rec, T mu, T lambda, T kappa,
                                         const ScalarState<T> &st, T Qm[3][3]) {
   T s[6];
 #pragma unroll

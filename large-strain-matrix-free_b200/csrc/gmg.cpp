@@ -655,6 +655,12 @@ lsmf_status lsmf_cg_solve(lsmf_op *A, int precond, double omega, lsmf_gmg *gmg, 
     set_error("a bounded device wait timed out in the vmult kernel");
     return LSMF_ERR_TIMEOUT;
   }
+  if (flag & 4) {
+    LSMF_CUDA(cudaMemsetAsync(A->d_flag.ptr, 0, sizeof(int), st));
+    LSMF_CUDA(cudaStreamSynchronize(st));
+    set_error("a vmult kernel was launched with less shared memory than its layout needs and did no work");
+    return LSMF_ERR_CUDA;
+  }
   if (!conv) {
     // the facts of deal.II's SolverControl::NoConvergence: last step and value
     char msg[160];

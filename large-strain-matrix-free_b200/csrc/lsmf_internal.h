@@ -194,6 +194,7 @@ struct lsmf_op {
   int max_warps = 0;                 // warps per block cap of the vmult kernel (<= 8, 0 auto)
   int wait_tries = -1;               // bulk-copy wait bound (try_wait calls; -1 = default 2^22)
   int prefetch = -1;                 // plain-load kernels: L1 prefetch of the record (0, 1 this cell, 2 next; -1 auto)
+  int pairs = -1;                    // FP32 vmult: two cells per warp in packed f32x2 arithmetic (0 off, 1 on, -1 auto)
   int device = 0;                    // CUDA device the operator's buffers live on
   int scatter = LSMF_SCATTER_ATOMIC; // cell-loop scatter: atomics or the 8 colour launches
   cudaStream_t stream = 0;

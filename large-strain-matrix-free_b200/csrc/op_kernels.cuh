@@ -18,6 +18,7 @@
 #include "cell_kernels.cuh"
 #include "lsmf_internal.h"
 #include "op_dispatch.h"
+#include "pair.cuh"
 
 namespace lsmf {
 
@@ -140,7 +141,10 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
-constexpr int FLAG_DETF = 1, FLAG_TIMEOUT = 2;
+// device error word bits: det F <= 0 at a point (cache), a bounded wait
+// ran out, a kernel found less dynamic shared memory than its layout needs
+// (it returned without touching memory)
+constexpr int FLAG_DETF = 1, FLAG_TIMEOUT = 2, FLAG_SMEM = 4;
 // internal stage bit: gather constrained entries instead of zeroing them
 constexpr unsigned MASK_INHOM = MASK_INHOM_BIT;
 
@@ -625,6 +629,210 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
   }
 }
 
+// ------------------------------------------------ FP32 cell-pair kernel
+// The plain-load cell loop of apply_fast_kernel for FP32 operators with two
+// cells per warp: list entries 2i and 2i + 1 go through the sweeps and the
+// point physics together as the two halves of packed f32x2 registers
+// (pair.cuh), so one issued arithmetic or shared-memory instruction serves
+// both cells.  Gathers, record loads and the scatter stay per cell.  With an
+// odd count the last pair repeats its first cell and scatters it once.
+// per-warp shared memory of the pair kernel (8 bytes, then the slab of the
+// 8-byte-entry sweep layout), used by the kernel and by its launcher
+template <int P, int Q>
+__host__ __device__ constexpr size_t pair_warp_bytes() {
+  return ((8 + SFR<P, Q, f2>::SZ * sizeof(f2) + 127) / 128) * 128;
+}
+
+template <int P, int Q, int VAR, bool COL>
+__global__ void __launch_bounds__(256) apply_pair_kernel(KArgs<float> a, TabT<P, Q, f2> tab) {
+  using T = f2;
+  constexpr bool SCALAR = (VAR == VAR_SCALAR_F0 || VAR == VAR_SCALAR_F1);
+  constexpr bool CLAMP = SCALAR || VAR == VAR_SCALAR_REF;
+  using S = SFR<P, Q, T, CLAMP>;
+  constexpr int N1 = P + 1, NN = S::NN, NQ = S::NQ, QPL = S::QPL, RPL = S::RPL, XR = S::XR;
+  constexpr bool PT_SMEM = !SCALAR && QPL >= 2;
+  const int WPB = blockDim.x >> 5;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int rec_elems = a.rec_elems;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr size_t warp_bytes = pair_warp_bytes<P, Q>();
+  {
+    // the launch must provide every warp's slab; otherwise do nothing
+    unsigned dyn;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+    if ((size_t)WPB * warp_bytes > dyn) {
+      if (threadIdx.x == 0) atomicOr(a.flag, FLAG_SMEM);
+      return;
+    }
+  }
+  T *slab = (T *)(smem + warp * warp_bytes + 8);
+  const int gw = blockIdx.x * WPB + warp, nw = gridDim.x * WPB;
+  const int n_pairs = (a.n_cells + 1) >> 1;
+  auto cid = [&](int i) -> int { return COL ? __ldg(a.cells + i) : i; };
+  // gather registers of the x rows (c, k, j) owned by this lane, both cells
+  int pk0[RPL][N1], pk1[RPL][N1];
+  float pv0[RPL][N1], pv1[RPL][N1], pu0[RPL][N1], pu1[RPL][N1];
+  auto prefetch = [&](int pi) {
+    const int e0 = 2 * pi, e1 = (2 * pi + 1 < a.n_cells) ? 2 * pi + 1 : 2 * pi;
+    const int *cn0 = a.cell_nodes + (size_t)cid(e0) * NN, *cn1 = a.cell_nodes + (size_t)cid(e1) * NN;
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int row = lane + 32 * r;
+      if ((CLAMP && XR <= 32) || row < XR) {
+        int comp, xk, xj;
+        S::x_row(row < XR ? row : XR - 1, comp, xk, xj);
+        const int kj = xk * N1 + xj;
+#pragma unroll
+        for (int i = 0; i < N1; ++i) {
+          const int k0 = __ldg(cn0 + kj * N1 + i), k1 = __ldg(cn1 + kj * N1 + i);
+          pk0[r][i] = k0;
+          pk1[r][i] = k1;
+          const size_t d0 = 3 * (size_t)(k0 & NODE_MASK) + comp, d1 = 3 * (size_t)(k1 & NODE_MASK) + comp;
+          pv0[r][i] = __ldg(a.src + d0);
+          pv1[r][i] = __ldg(a.src + d1);
+          if (SCALAR) {
+            pu0[r][i] = __ldg(a.u + d0);
+            pu1[r][i] = __ldg(a.u + d1);
+          }
+        }
+      }
+    }
+  };
+  if (gw < n_pairs) prefetch(gw);
+  for (int pi = gw; pi < n_pairs; pi += nw) {
+    const int e0 = 2 * pi;
+    const bool two = 2 * pi + 1 < a.n_cells;
+    const int e1 = two ? e0 + 1 : e0;
+    const int c0 = cid(e0), c1 = cid(e1);
+    int ck0[RPL][N1], ck1[RPL][N1];
+    T v[RPL][N1], vu[RPL][N1];
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int row = lane + 32 * r;
+      int comp = 0, xk, xj;
+      if ((CLAMP && XR <= 32) || row < XR) S::x_row(row < XR ? row : XR - 1, comp, xk, xj);
+      if (!(CLAMP && XR <= 32) && row >= XR) {
+#pragma unroll
+        for (int i = 0; i < N1; ++i) { ck0[r][i] = 0; ck1[r][i] = 0; v[r][i] = T(0); vu[r][i] = T(0); }
+        continue;
+      }
+#pragma unroll
+      for (int i = 0; i < N1; ++i) {
+        ck0[r][i] = pk0[r][i];
+        ck1[r][i] = pk1[r][i];
+        // read_dof_values(src): constrained entries read as zero
+        v[r][i] = pack2(((pk0[r][i] >> (NODE_BITS + comp)) & 1) ? 0.f : pv0[r][i],
+                        ((pk1[r][i] >> (NODE_BITS + comp)) & 1) ? 0.f : pv1[r][i]);
+        if (SCALAR) vu[r][i] = pack2(pu0[r][i], pu1[r][i]);
+      }
+    }
+    if (pi + nw < n_pairs) prefetch(pi + nw);
+    if (a.prefetch) {
+      // both records into L1 before the sweeps
+      const char *b0 = (const char *)(a.table + (size_t)c0 * rec_elems);
+      const char *b1 = (const char *)(a.table + (size_t)c1 * rec_elems);
+      const int nbytes = rec_elems * (int)sizeof(float);
+      for (int off = lane * 128; off < nbytes; off += 32 * 128) {
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(b0 + off));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(b1 + off));
+      }
+    }
+    T G[QPL][3][3], GU[QPL][3][3];
+    if (SCALAR) S::eval(tab, vu, slab, lane, GU);
+    if (PT_SMEM) S::eval_pt(tab, v, slab, lane);
+    else S::eval(tab, v, slab, lane, G);
+    const RecPair rec{a.table + (size_t)c0 * rec_elems, a.table + (size_t)c1 * rec_elems};
+    T mu = 0, lambda = 0, kappa = 0;
+    if (SCALAR || VAR == VAR_SCALAR_REF) {
+      float m0, l0, k0, m1, l1, k1;
+      material<float>(a.mu[c0], a.nu, m0, l0, k0);
+      material<float>(a.mu[c1], a.nu, m1, l1, k1);
+      mu = pack2(m0, m1);
+      lambda = pack2(l0, l1);
+      kappa = pack2(k0, k1);
+    }
+    T H[QPL][3][3];
+#pragma unroll(PT_SMEM ? 1 : QPL)
+    for (int l = 0; l < QPL; ++l) {
+      const int q = (CLAMP && NQ <= 32) ? (lane < NQ ? lane : NQ - 1) : lane + 32 * l;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int e = 0; e < 3; ++e) H[l][c][e] = T(0);
+      if (!(CLAMP && NQ <= 32) && q >= NQ) continue;
+      const RecPair r = rec + q;
+      T Ji[3][3];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) Ji[i / 3][i % 3] = r[(C_JINV + i) * NQ];
+      const T jxw = r[C_JXW * NQ];
+      T Gq[3][3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int e = 0; e < 3; ++e) Gq[c][e] = PT_SMEM ? slab[(c * 3 + e) * S::NQP + q] : G[l][c][e];
+      T g[3][3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) g[c][d] = Gq[c][0] * Ji[0][d] + Gq[c][1] * Ji[1][d] + Gq[c][2] * Ji[2][d];
+      ScalarState<T> st;
+      if (SCALAR) {
+        T Jr[3][3];
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+          Jr[i / 3][i % 3] = a.ref_per_cell ? rec[(C_VAR + 1) * NQ + i] : r[(C_VAR + 1 + i) * NQ];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            st.F[c][d] = GU[l][c][0] * Jr[0][d] + GU[l][c][1] * Jr[1][d] + GU[l][c][2] * Jr[2][d] + (c == d ? T(1) : T(0));
+        st.det = det3(st.F);
+      }
+      if (VAR == VAR_SCALAR_REF) {
+        collocation_F<Q>(rec, q, tab.Dc, Ji, st.F);
+        st.det = det3(st.F);
+      }
+      T Qm[3][3];
+      physics<T, VAR, NQ>(g, r, mu, lambda, kappa, st, Qm);
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+          const T h = (Qm[c][0] * Ji[e][0] + Qm[c][1] * Ji[e][1] + Qm[c][2] * Ji[e][2]) * jxw;
+          if (PT_SMEM) slab[(c * 3 + e) * S::NQP + q] = h;
+          else H[l][c][e] = h;
+        }
+    }
+    T out[RPL][N1];
+    if (PT_SMEM) S::integrate_pt(tab, slab, lane, out);
+    else S::integrate(tab, H, slab, lane, out);
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int row = lane + 32 * r;
+      if (row < XR) {
+        int comp, xk, xj;
+        S::x_row(row, comp, xk, xj);
+#pragma unroll
+        for (int i = 0; i < N1; ++i) {
+          float o0, o1;
+          unpack2(out[r][i], o0, o1);
+          // distribute_local_to_global: constrained rows skipped
+          if (!((ck0[r][i] >> (NODE_BITS + comp)) & 1)) {
+            float *d = a.dst + 3 * (size_t)(ck0[r][i] & NODE_MASK) + comp;
+            if (COL) *d += o0;
+            else atomicAdd(d, o0);
+          }
+          if (two && !((ck1[r][i] >> (NODE_BITS + comp)) & 1)) {
+            float *d = a.dst + 3 * (size_t)(ck1[r][i] & NODE_MASK) + comp;
+            if (COL) *d += o1;
+            else atomicAdd(d, o1);
+          }
+        }
+      }
+    }
+  }
+}
+
 // --------------------------------------------------------- diagonal kernel
 // diag(a,c) = sum_q JxW n^T B_c n with n = grad_x N_a and
 // B_c[d][l] = Q(e_c (x) e_l)[c][d]: identical to applying the cell operator
@@ -897,6 +1105,35 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
   // the colour launches are built with at most one stage
   const bool col = a.cells != nullptr;
   if (col && stages > 1) stages = 1;
+  if constexpr (std::is_same<T, float>::value) {
+    // automatic choice, measured on B200 (FP32 vmult at 96^3 Q1, 64^3 Q2,
+    // 48^3 Q3 / Q4 and the 15^3 -> 30^3 / 60^3 Q2 V-cycles), pairs where
+    // they were faster: Q1 tensor2 (-2 %) and scalar (-8 %); Q2 tensor2
+    // (-9 %, V-cycle -5 %), scalar (-8 %, V-cycle -7 %) and
+    // scalar_referential (-11 %); Q4 scalar_referential (-10 %).  Every Q3
+    // variant (+5-13 %), the record-heavy tensor4 (Q2 +27 %) and tensor4_ns
+    // (+8 %), whose loops are bound by load latency and lose half their warps
+    // to the pair kernel's registers, and formulation 0 (+12 %, 159
+    // registers) stay one cell per warp.
+    constexpr bool pair_variant = (P == 1 && (VAR == VAR_TENSOR2 || VAR == VAR_SCALAR_F1)) ||
+                                  (P == 2 && (VAR == VAR_TENSOR2 || VAR == VAR_SCALAR_F1 || VAR == VAR_SCALAR_REF)) ||
+                                  (P == 4 && VAR == VAR_SCALAR_REF);
+    if (full && !op->basic && (op->pairs > 0 || (op->pairs < 0 && pair_variant))) {
+      // FP32 cell pairs (plain loads; the ring is not used)
+      const size_t wb = pair_warp_bytes<P, Q>();
+      const int w = warps_for_budget(wb, max_warps < 8 ? max_warps : 8, 220 * 1024);
+      const size_t smem_p = w * wb;
+      const TabT<P, Q, f2> tabp = make_tabt<P, Q, f2>(op->mesh->basis);
+      const int n_pairs = (a.n_cells + 1) / 2;
+      auto go = [&](auto k) -> lsmf_status {
+        LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_p));
+        const int g = grid_for(k, 32 * w, smem_p, (n_pairs + w - 1) / w);
+        k<<<g, 32 * w, smem_p, op->stream>>>(a, tabp);
+        return LSMF_OK;
+      };
+      return col ? go(apply_pair_kernel<P, Q, VAR, true>) : go(apply_pair_kernel<P, Q, VAR, false>);
+    }
+  }
   if (full && !op->basic) {
     // at most 8 warps per block (the kernel's launch bound is 256 threads);
     // smaller blocks let several blocks share an SM

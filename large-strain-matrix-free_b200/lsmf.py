@@ -344,6 +344,18 @@ class NeoHookOperator:
         bit-reproducible)."""
         check(lib().lsmf_operator_set_option(self.h, 5, SCATTER[mode] if isinstance(mode, str) else int(mode)))
 
+    def set_record_prefetch(self, mode):
+        """L1 prefetch of the cell record with plain loads: 0 none, 1 this
+        cell's, 2 the next cell's, -1 the measured default."""
+        check(lib().lsmf_operator_set_option(self.h, 6, int(mode)))
+
+    def set_cell_pairs(self, mode):
+        """FP32 operators: 1 = two cells per warp in packed f32x2 arithmetic,
+        0 = one cell per warp, -1 = the measured default (pairs for Q1
+        tensor2 / scalar, Q2 tensor2 / scalar / scalar_referential, Q4
+        scalar_referential; formulation 1)."""
+        check(lib().lsmf_operator_set_option(self.h, 7, int(mode)))
+
     def sync(self):
         """Wait for the operator's stream; raises LsmfError (status 8) if a
         bounded device wait ran out since the last call."""

@@ -49,12 +49,17 @@ VARIANTS = [("tensor4", 1), ("tensor2", 1), ("scalar", 1), ("scalar", 0), ("scal
 
 
 KERNELS = ["bulk1", "bulk2", "bulk3", "plain", "basic"]
+# FP32 also has the cell-pair kernel (two cells per warp, packed f32x2)
+KERNELS32 = KERNELS + ["pairs"]
 
 
 def _select(op, kernel):
+    # the one-cell kernels are selected with pairs off (the default turns
+    # them on for some FP32 variants; FP64 operators ignore the option)
+    op.set_cell_pairs(1 if kernel == "pairs" else 0)
     if kernel == "basic":
         op.set_basic_kernel(True)
-    else:
+    elif kernel != "pairs":
         op.set_pipeline({"bulk1": 1, "bulk2": 2, "bulk3": 3, "plain": 0}[kernel])
 
 
@@ -84,7 +89,7 @@ def test_vmult_fp64_matches_oracle(caching, formulation, p, kernel):
 
 @pytest.mark.parametrize("caching,formulation", VARIANTS)
 @pytest.mark.parametrize("p", [1, 2, 3, 4])
-@pytest.mark.parametrize("kernel", KERNELS)
+@pytest.mark.parametrize("kernel", KERNELS32)
 def test_vmult_fp32_matches_oracle(caching, formulation, p, kernel):
     gm, om, cmask, mu, u, src = _setup(p=p, coarse=(2, 2, 2) if p < 4 else (1, 2, 1), level=1)
     ref = _oracle_op(om, cmask, mu, u, caching, formulation)
