@@ -138,7 +138,8 @@ lsmf_status lsmf_operator_el(lsmf_op *op, int row, int col, double *value);
  * LSMF_OPT_BULK_PIPELINE: depth 1..3 of the shared-memory ring through which
  *   each warp streams its cell records with bulk copies; 0 = plain coalesced
  *   loads; -1 (default) = measured choice: 1 for tensor4, tensor4_ns and
- *   scalar_referential while a cell record fits in 24 KB, else 0.  The
+ *   scalar_referential of degree 1 or 2 while a cell record fits in 24 KB,
+ *   else 0.  The
  *   depth is reduced when the ring would not fit in shared memory.
  * LSMF_OPT_BASIC_KERNEL: 1 = the basic vmult kernel (per-warp shared-memory
  *   sweeps, plain loads); the stage mask of vmult always uses it.

@@ -1084,15 +1084,18 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
   const size_t rec_bytes = (size_t)op->rec_elems * sizeof(T);
   const TabT<P, Q, T> tabt = make_tabt<P, Q, T>(op->mesh->basis);
   auto wbytes = [&](int st) { return ((st * rec_bytes + 8 * (st > 0 ? st : 1) + SR::SZ * sizeof(T) + 127) / 128) * 128; };
-  // defaults measured on B200 (ring depth x warps per block swept for
-  // Q2 / Q3 / Q4 at 64^3 / 48^3 / 48^3 cells): the variants that stream a
-  // large record per point (tensor4, tensor4_ns) and scalar_referential
-  // (whose collocation gradient reads the record out of order) want the
-  // one-stage bulk-copy ring while a record fits in 24 KB; larger records
-  // (Q3 FP64, Q4) cost more occupancy than the ring gains and run on plain
-  // loads, as do tensor2 and scalar (latency / FP64 bound)
+  // defaults measured on B200 (ring depth x record prefetch x warps per
+  // block swept for Q2 / Q3 / Q4 at 64^3 / 48^3 / 48^3 cells): at Q1 / Q2
+  // the variants that stream a large record per point (tensor4, tensor4_ns)
+  // and scalar_referential (whose collocation gradient reads the record out
+  // of order) want the one-stage bulk-copy ring while a record fits in
+  // 24 KB; from Q3 on, plain loads with the L1 record prefetch are faster
+  // (Q3 FP32 tensor4 0.409 -> 0.337 ms, tensor4_ns 0.661 -> 0.449 ms,
+  // scalar_referential FP32 -6 % / FP64 -15 %), as they are for the larger
+  // records (Q3 FP64 tensor4, Q4) and for tensor2 and scalar (latency / FP64
+  // bound)
   const bool ring_variant = VAR == VAR_TENSOR4 || VAR == VAR_TENSOR4_NS || VAR == VAR_SCALAR_REF;
-  int stages = op->stages >= 0 ? op->stages : ((ring_variant && rec_bytes <= 24 * 1024) ? 1 : 0);
+  int stages = op->stages >= 0 ? op->stages : ((ring_variant && P <= 2 && rec_bytes <= 24 * 1024) ? 1 : 0);
   // a level small enough that every warp gets at most one cell (a coarse
   // multigrid level) gains nothing from the ring, which can only prefetch
   // a warp's next cell: plain loads (15^3-cell FP64 coarse Chebyshev solve

@@ -321,7 +321,8 @@ class NeoHookOperator:
     def set_pipeline(self, stages):
         """Ring depth (0..3) of the bulk-copy record pipeline in vmult; 0 =
         plain loads, -1 = the measured default (one stage for the large-record
-        variants while a record fits in 24 KB, else plain loads).  True/False
+        variants of degree 1 or 2 while a record fits in 24 KB, else plain
+        loads).  True/False
         select 2/0."""
         if stages is True:
             stages = 2
