@@ -155,7 +155,13 @@ lsmf_status lsmf_operator_el(lsmf_op *op, int row, int col, double *value);
  *   cells are processed in the 8 parity colours of the structured lattice,
  *   one launch per colour, so that no two cells of a launch share a node
  *   and the sums are formed in a fixed order without atomics
- *   (bit-reproducible vmult, for parity and debugging).
+ *   (bit-reproducible vmult, for parity and debugging); 2 = nodesum: one
+ *   full cell loop stores every cell's results to a per-cell buffer
+ *   (n_cells x 3 (p+1)^3 values, allocated when the mode is selected) and
+ *   a node kernel adds each node's cell contributions in increasing cell
+ *   order (bit-reproducible as well, one cell loop instead of eight; the
+ *   diagonal and the other cell loops of a nodesum operator use the
+ *   colours).
  * LSMF_OPT_RECORD_PREFETCH: with plain record loads, 1 issues an L1
  *   prefetch of the cell's record before its sum-factorisation sweeps, 2 of
  *   the next cell's record, 0 none; -1 (default): 1, except 0 for the FP64
@@ -172,7 +178,7 @@ lsmf_status lsmf_operator_el(lsmf_op *op, int row, int col, double *value);
  * set-up (the next synchronising call on the operator). */
 enum { LSMF_OPT_BULK_PIPELINE = 1, LSMF_OPT_BASIC_KERNEL = 2, LSMF_OPT_MAX_WARPS = 3, LSMF_OPT_WAIT_TRIES = 4,
        LSMF_OPT_SCATTER = 5, LSMF_OPT_RECORD_PREFETCH = 6, LSMF_OPT_CELL_PAIRS = 7 };
-enum { LSMF_SCATTER_ATOMIC = 0, LSMF_SCATTER_COLOUR8 = 1 };
+enum { LSMF_SCATTER_ATOMIC = 0, LSMF_SCATTER_COLOUR8 = 1, LSMF_SCATTER_NODESUM = 2 };
 lsmf_status lsmf_operator_set_option(lsmf_op *op, int option, int value);
 /* Wait for the operator's stream and report a device error its kernels
  * recorded since the last report (LSMF_ERR_TIMEOUT for a bounded wait that

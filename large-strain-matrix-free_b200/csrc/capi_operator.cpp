@@ -250,14 +250,7 @@ lsmf_status lsmf_operator_set_option(lsmf_op *op, int option, int value) {
     op->pairs = value;
     return LSMF_OK;
   }
-  if (option == LSMF_OPT_SCATTER) {
-    if (value != LSMF_SCATTER_ATOMIC && value != LSMF_SCATTER_COLOUR8) {
-      set_error("scatter must be 0 (atomic) or 1 (colour8)");
-      return LSMF_ERR_INVALID_ARG;
-    }
-    op->scatter = value;
-    return LSMF_OK;
-  }
+  if (option == LSMF_OPT_SCATTER) return set_scatter_mode(op, value);
   set_error("unknown option");
   return LSMF_ERR_INVALID_ARG;
 }

@@ -501,12 +501,10 @@ lsmf_status lsmf_gmg_set_option(lsmf_gmg *g, int option, int value) {
     return LSMF_OK;
   }
   if (option == LSMF_GMG_OPT_SCATTER) {
-    if (value != LSMF_SCATTER_ATOMIC && value != LSMF_SCATTER_COLOUR8) {
-      set_error("scatter must be 0 (atomic) or 1 (colour8)");
-      return LSMF_ERR_INVALID_ARG;
-    }
+    // level operators take the mode (node sums for their vmult cell loops);
+    // transfers run the colours for every mode but atomic
+    for (auto &GL : g->levels) LSMF_TRY(set_scatter_mode(GL.op, value));
     g->scatter = value;
-    for (auto &GL : g->levels) GL.op->scatter = value;
     // the captured V-cycle holds the old launch sequence
     drop_graph(g);
     return LSMF_OK;

@@ -5,8 +5,10 @@
 // ops_for().
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "cell_kernels.cuh"
 #include "lsmf_internal.h"
@@ -57,6 +59,30 @@ const OpsTable *table_of(const lsmf_op *op) {
   return t;
 }
 
+// node-sum scatter: dst (+)= the sum over the node's cells, in increasing
+// cell order, of the node's slot in the per-cell buffer (a fixed order: the
+// result is the same from call to call)
+template <typename T>
+__global__ void node_sum_kernel(T *dst, const T *__restrict__ buf, const int *__restrict__ off,
+                                const int *__restrict__ ent, int n_nodes, int add) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_nodes; n += gridDim.x * blockDim.x) {
+    T s0 = 0, s1 = 0, s2 = 0;
+    const int e1 = __ldg(off + n + 1);
+    for (int e = __ldg(off + n); e < e1; ++e) {
+      const int b = __ldg(ent + e);
+      s0 += buf[b];
+      s1 += buf[b + 1];
+      s2 += buf[b + 2];
+    }
+    T *d = dst + 3 * (size_t)n;
+    if (add) {
+      d[0] += s0; d[1] += s1; d[2] += s2;
+    } else {
+      d[0] = s0; d[1] = s1; d[2] = s2;
+    }
+  }
+}
+
 }  // namespace
 
 // Components per quadrature point of the cell record.  The FP32 tensor2
@@ -84,7 +110,9 @@ lsmf_status launch_cache(lsmf_op *op) {
 // its cell contributions in the same order on every call).
 template <typename F>
 lsmf_status for_cell_ranges(const Level &L, int scatter, F &&f) {
-  if (scatter == LSMF_SCATTER_COLOUR8) {
+  // the node-sum scatter serves the full vmult cell loop; every other cell
+  // loop of a node-sum operator runs the (equally deterministic) colours
+  if (scatter != LSMF_SCATTER_ATOMIC) {
     for (int c = 0; c < 8; ++c) {
       CellRange r;
       r.cells = L.d_colour_cells.ptr + L.colour_off[c];
@@ -97,13 +125,76 @@ lsmf_status for_cell_ranges(const Level &L, int scatter, F &&f) {
   return f(CellRange{});
 }
 
+// the node-sum path applies: the operator asks for it and the launch is the
+// full production cell loop
+static bool node_sum_path(const lsmf_op *op, unsigned mask) {
+  const unsigned all = LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD;
+  return op->scatter == LSMF_SCATTER_NODESUM && !op->basic && (mask & all) == all && !(mask & MASK_INHOM_BIT);
+}
+
+// cell loop into the operator's cell buffer, then dst (+)= node sums
+static lsmf_status apply_node_sum(const lsmf_op *op, const OpsTable *t, void *dst, const void *src, unsigned mask,
+                                  bool add) {
+  const Level &L = op->L();
+  if (!op->d_cellbuf.ptr || !L.d_node_cell_off.ptr) {
+    set_error("node-sum scatter selected without its buffers");
+    return LSMF_ERR_NOT_INITIALIZED;
+  }
+  CellRange r;
+  r.cellbuf = op->d_cellbuf.ptr;
+  LSMF_TRY(t->apply(op, dst, src, mask, r));
+  const int g = std::min((L.n_nodes + 255) / 256, 8 * num_sms());
+  if (op->precision == LSMF_FP64)
+    node_sum_kernel<double><<<g, 256, 0, op->stream>>>((double *)dst, (const double *)op->d_cellbuf.ptr,
+                                                      L.d_node_cell_off.ptr, L.d_node_cell_ent.ptr, L.n_nodes, add);
+  else
+    node_sum_kernel<float><<<g, 256, 0, op->stream>>>((float *)dst, (const float *)op->d_cellbuf.ptr,
+                                                     L.d_node_cell_off.ptr, L.d_node_cell_ent.ptr, L.n_nodes, add);
+  LSMF_CUDA(cudaGetLastError());
+  return LSMF_OK;
+}
+
+lsmf_status set_scatter_mode(lsmf_op *op, int mode) {
+  if (mode != LSMF_SCATTER_ATOMIC && mode != LSMF_SCATTER_COLOUR8 && mode != LSMF_SCATTER_NODESUM) {
+    set_error("scatter must be 0 (atomic), 1 (colour8) or 2 (nodesum)");
+    return LSMF_ERR_INVALID_ARG;
+  }
+  if (mode == LSMF_SCATTER_NODESUM) {
+    Level &L = op->L();
+    const int ncn = L.ncn();
+    if ((double)L.n_cells * ncn * 3 > 2147483647.0) {
+      set_error("the node-sum scatter indexes its cell buffer with 32-bit offsets; this level is too large");
+      return LSMF_ERR_UNSUPPORTED;
+    }
+    if (!L.d_node_cell_off.ptr) {
+      // counting sort of the (cell, local node) slots by node, cells in
+      // increasing order within a node
+      std::vector<int> off(L.n_nodes + 1, 0), ent((size_t)L.n_cells * ncn);
+      for (size_t k = 0; k < ent.size(); ++k) ++off[L.cell_nodes[k] + 1];
+      for (int n = 0; n < L.n_nodes; ++n) off[n + 1] += off[n];
+      std::vector<int> pos(off.begin(), off.end() - 1);
+      for (int c = 0; c < L.n_cells; ++c)
+        for (int a = 0; a < ncn; ++a) ent[pos[L.cell_nodes[(size_t)c * ncn + a]]++] = (c * ncn + a) * 3;
+      LSMF_TRY(L.d_node_cell_off.upload(off.data(), off.size()));
+      LSMF_TRY(L.d_node_cell_ent.upload(ent.data(), ent.size()));
+    }
+    LSMF_TRY(op->d_cellbuf.alloc((size_t)L.n_cells * ncn * 3 * op->elem()));
+  }
+  op->scatter = mode;
+  return LSMF_OK;
+}
+
 lsmf_status launch_apply(const lsmf_op *op, void *dst, const void *src, unsigned mask, bool add) {
   const Level &L = op->L();
   const OpsTable *t = table_of(op);
   if (!t) return LSMF_ERR_UNSUPPORTED;
   const size_t n = (size_t)L.n_dofs();
-  if (!add && (mask & LSMF_MASK_ZERO)) LSMF_CUDA(cudaMemsetAsync(dst, 0, n * op->elem(), op->stream));
-  LSMF_TRY(for_cell_ranges(L, op->scatter, [&](CellRange r) { return t->apply(op, dst, src, mask, r); }));
+  if (node_sum_path(op, mask)) {
+    LSMF_TRY(apply_node_sum(op, t, dst, src, mask, add || !(mask & LSMF_MASK_ZERO)));
+  } else {
+    if (!add && (mask & LSMF_MASK_ZERO)) LSMF_CUDA(cudaMemsetAsync(dst, 0, n * op->elem(), op->stream));
+    LSMF_TRY(for_cell_ranges(L, op->scatter, [&](CellRange r) { return t->apply(op, dst, src, mask, r); }));
+  }
   // constrained rows: dst += src (mf_nh_operator.h:702-705)
   const int nc = (int)L.constrained.size();
   if (nc && (mask & LSMF_MASK_RW)) {
@@ -121,6 +212,7 @@ lsmf_status launch_apply_cells(const lsmf_op *op, void *dst, const void *src) {
   const OpsTable *t = table_of(op);
   if (!t) return LSMF_ERR_UNSUPPORTED;
   const unsigned mask = LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD;
+  if (node_sum_path(op, mask)) return apply_node_sum(op, t, dst, src, mask, true);
   return for_cell_ranges(op->L(), op->scatter, [&](CellRange r) { return t->apply(op, dst, src, mask, r); });
 }
 

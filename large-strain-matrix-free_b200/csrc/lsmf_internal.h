@@ -117,6 +117,11 @@ struct Level {
   std::vector<int> colour_cells;
   int colour_off[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   DevBuf<int> d_colour_cells;
+  // node -> its cells, for the node-sum scatter (built on first use): the
+  // entries of node n are node_cell_off[n] .. node_cell_off[n+1], each the
+  // offset (cell * ncn + local node) * 3 of the node's slot in a per-cell
+  // buffer [cell][local node][component], in increasing cell order
+  DevBuf<int> d_node_cell_off, d_node_cell_ent;
   // device
   DevBuf<int> d_cell_nodes;     // packed with constraint bits
   DevBuf<double> d_X;
@@ -196,7 +201,8 @@ struct lsmf_op {
   int prefetch = -1;                 // plain-load kernels: L1 prefetch of the record (0, 1 this cell, 2 next; -1 auto)
   int pairs = -1;                    // FP32 vmult: two cells per warp in packed f32x2 arithmetic (0 off, 1 on, -1 auto)
   int device = 0;                    // CUDA device the operator's buffers live on
-  int scatter = LSMF_SCATTER_ATOMIC; // cell-loop scatter: atomics or the 8 colour launches
+  int scatter = LSMF_SCATTER_ATOMIC; // cell-loop scatter: atomics, the 8 colour launches, or node sums
+  lsmf::DevBuf<char> d_cellbuf;      // node-sum scatter: per-cell results [cell][local node][component]
   cudaStream_t stream = 0;
   // CG workspace (outer FP64 CG driven through this operator)
   lsmf::DevBuf<double> cg_g, cg_h, cg_d, sc, partial;
@@ -212,6 +218,10 @@ lsmf_status launch_apply(const lsmf_op *op, void *dst, const void *src, unsigned
 // identity rows); callers fold those into their own element-wise kernels
 lsmf_status launch_apply_cells(const lsmf_op *op, void *dst, const void *src);
 lsmf_status launch_diagonal(lsmf_op *op);
+// select the cell-loop scatter of an operator (LSMF_SCATTER_*); the
+// node-sum mode builds the level's node -> cell lists and the operator's
+// cell buffer on first use
+lsmf_status set_scatter_mode(lsmf_op *op, int mode);
 lsmf_status upload_basis_tables(const Basis &b);
 int table_components(int caching, int formulation, lsmf_precision precision);
 }  // namespace lsmf

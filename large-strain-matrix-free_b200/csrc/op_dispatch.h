@@ -9,11 +9,14 @@ namespace lsmf {
 // A cell loop runs over `cells[0 .. n_list)` when `cells` is given (one
 // colour of the lattice: no two listed cells share a node, so the scatter
 // is a plain read-modify-write), else over all cells of the level with
-// atomic scatter.
+// atomic scatter, or, with `cellbuf` (full vmult cell loop only), storing
+// every cell's results to cellbuf[cell][local node][component] for a node
+// sum that follows.
 struct CellRange {
   const int *cells = nullptr;
   int n_list = 0;
   bool plain = false;
+  void *cellbuf = nullptr;
 };
 
 struct OpsTable {

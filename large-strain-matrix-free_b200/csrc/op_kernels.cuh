@@ -44,6 +44,7 @@ struct KArgs {
   int prefetch;          // plain loads: L1 prefetch of the record (0 off, 1 this cell, 2 the next cell)
   const int *cells;      // cell list of one colour (nullptr: all n_cells cells)
   int plain;             // scatter with plain adds (colour launches) instead of atomics
+  T *cellbuf;            // node-sum scatter: per-cell results [cell][local node][component]
 };
 
 // cell of list entry i
@@ -400,12 +401,16 @@ __global__ void __launch_bounds__(256) apply_kernel(KArgs<T> a, Tab<P, Q> tab) {
 // prefetched into registers while the current cell is computed; with
 // STAGES == 2 each warp streams its cell records through a two-stage
 // shared-memory ring filled by cp.async.bulk (evict-first in L2), with
-// STAGES == 0 the record is read with plain coalesced loads.  COL: the
-// loop runs over the cell list of one lattice colour (a.cells, a.n_cells
-// entries) and scatters with plain adds; otherwise over all cells with
-// atomics.
-template <int P, int Q, typename T, int VAR, int STAGES, bool COL>
+// STAGES == 0 the record is read with plain coalesced loads.  SC (scatter):
+// SC_ATOMIC loops over all cells and adds with atomics; SC_COLOUR over the
+// cell list of one lattice colour (a.cells, a.n_cells entries) with plain
+// adds; SC_CELLBUF over all cells, storing every cell's results to
+// a.cellbuf[cell][local node][component] (constrained rows as zero) for the
+// node sum that follows.
+constexpr int SC_ATOMIC = 0, SC_COLOUR = 1, SC_CELLBUF = 2;
+template <int P, int Q, typename T, int VAR, int STAGES, int SC>
 __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, T> tab) {
+  constexpr bool COL = SC == SC_COLOUR;
   constexpr bool SCALAR = (VAR == VAR_SCALAR_F0 || VAR == VAR_SCALAR_F1);
   // branch-free sweeps and point loop for the scalar variants (48^3 / 64^3
   // Q2: scalar -7 % FP64 / -10 % FP32, scalar_referential -4 % / -17 %;
@@ -618,7 +623,10 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
 #pragma unroll
         for (int i = 0; i < N1; ++i) {
           // distribute_local_to_global: constrained rows skipped
-          if (!((ck[r][i] >> (NODE_BITS + comp)) & 1)) {
+          const bool con = (ck[r][i] >> (NODE_BITS + comp)) & 1;
+          if (SC == SC_CELLBUF) {
+            a.cellbuf[((size_t)cell * NN + (xk * N1 + xj) * N1 + i) * 3 + comp] = con ? T(0) : out[r][i];
+          } else if (!con) {
             T *d = a.dst + 3 * (size_t)(ck[r][i] & NODE_MASK) + comp;
             if (COL) *d += out[r][i];
             else atomic_add(d, out[r][i]);
@@ -643,9 +651,10 @@ __host__ __device__ constexpr size_t pair_warp_bytes() {
   return ((8 + SFR<P, Q, f2>::SZ * sizeof(f2) + 127) / 128) * 128;
 }
 
-template <int P, int Q, int VAR, bool COL>
+template <int P, int Q, int VAR, int SC>
 __global__ void __launch_bounds__(256) apply_pair_kernel(KArgs<float> a, TabT<P, Q, f2> tab) {
   using T = f2;
+  constexpr bool COL = SC == SC_COLOUR;
   constexpr bool SCALAR = (VAR == VAR_SCALAR_F0 || VAR == VAR_SCALAR_F1);
   constexpr bool CLAMP = SCALAR || VAR == VAR_SCALAR_REF;
   using S = SFR<P, Q, T, CLAMP>;
@@ -817,15 +826,22 @@ __global__ void __launch_bounds__(256) apply_pair_kernel(KArgs<float> a, TabT<P,
           float o0, o1;
           unpack2(out[r][i], o0, o1);
           // distribute_local_to_global: constrained rows skipped
-          if (!((ck0[r][i] >> (NODE_BITS + comp)) & 1)) {
-            float *d = a.dst + 3 * (size_t)(ck0[r][i] & NODE_MASK) + comp;
-            if (COL) *d += o0;
-            else atomicAdd(d, o0);
-          }
-          if (two && !((ck1[r][i] >> (NODE_BITS + comp)) & 1)) {
-            float *d = a.dst + 3 * (size_t)(ck1[r][i] & NODE_MASK) + comp;
-            if (COL) *d += o1;
-            else atomicAdd(d, o1);
+          const bool con0 = (ck0[r][i] >> (NODE_BITS + comp)) & 1, con1 = (ck1[r][i] >> (NODE_BITS + comp)) & 1;
+          if (SC == SC_CELLBUF) {
+            const int local = (xk * N1 + xj) * N1 + i;
+            a.cellbuf[((size_t)e0 * NN + local) * 3 + comp] = con0 ? 0.f : o0;
+            if (two) a.cellbuf[((size_t)e1 * NN + local) * 3 + comp] = con1 ? 0.f : o1;
+          } else {
+            if (!con0) {
+              float *d = a.dst + 3 * (size_t)(ck0[r][i] & NODE_MASK) + comp;
+              if (COL) *d += o0;
+              else atomicAdd(d, o0);
+            }
+            if (two && !con1) {
+              float *d = a.dst + 3 * (size_t)(ck1[r][i] & NODE_MASK) + comp;
+              if (COL) *d += o1;
+              else atomicAdd(d, o1);
+            }
           }
         }
       }
@@ -1032,6 +1048,7 @@ KArgs<T> make_args(const lsmf_op *op) {
   a.wait_tries = op->wait_tries >= 0 ? op->wait_tries : WAIT_TRIES_DEFAULT;
   a.cells = nullptr;
   a.plain = 0;
+  a.cellbuf = nullptr;
   a.prefetch = op->prefetch;
   return a;
 }
@@ -1043,6 +1060,7 @@ void set_range(KArgs<T> &a, const CellRange &r) {
     a.n_cells = r.n_list;
   }
   a.plain = r.plain ? 1 : 0;
+  a.cellbuf = (T *)r.cellbuf;
 }
 
 template <int P, int Q, typename T, int VAR>
@@ -1105,9 +1123,14 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
   if (rec_bytes % 16 != 0) stages = 0;
   // fewer stages when the ring would leave fewer than 4 warps per block
   while (stages > 0 && warps_for_budget(wbytes(stages), 8, 220 * 1024) < 4) --stages;
-  // the colour launches are built with at most one stage
   const bool col = a.cells != nullptr;
-  if (col && stages > 1) stages = 1;
+  const bool cellbuf = a.cellbuf != nullptr;
+  if (cellbuf && !(full && !op->basic)) {
+    set_error("the node-sum scatter serves the full vmult cell loop only");
+    return LSMF_ERR_INVALID_ARG;
+  }
+  // the colour and cell-buffer launches are built with at most one stage
+  if ((col || cellbuf) && stages > 1) stages = 1;
   if constexpr (std::is_same<T, float>::value) {
     // automatic choice, measured on B200 (FP32 vmult at 96^3 Q1, 64^3 Q2,
     // 48^3 Q3 / Q4 and the 15^3 -> 30^3 / 60^3 Q2 V-cycles), pairs where
@@ -1134,7 +1157,9 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
         k<<<g, 32 * w, smem_p, op->stream>>>(a, tabp);
         return LSMF_OK;
       };
-      return col ? go(apply_pair_kernel<P, Q, VAR, true>) : go(apply_pair_kernel<P, Q, VAR, false>);
+      if (col) return go(apply_pair_kernel<P, Q, VAR, SC_COLOUR>);
+      if (cellbuf) return go(apply_pair_kernel<P, Q, VAR, SC_CELLBUF>);
+      return go(apply_pair_kernel<P, Q, VAR, SC_ATOMIC>);
     }
   }
   if (full && !op->basic) {
@@ -1150,13 +1175,17 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
       return LSMF_OK;
     };
     if (col) {
-      st = stages == 0 ? go(apply_fast_kernel<P, Q, T, VAR, 0, true>) : go(apply_fast_kernel<P, Q, T, VAR, 1, true>);
+      st = stages == 0 ? go(apply_fast_kernel<P, Q, T, VAR, 0, SC_COLOUR>)
+                       : go(apply_fast_kernel<P, Q, T, VAR, 1, SC_COLOUR>);
+    } else if (cellbuf) {
+      st = stages == 0 ? go(apply_fast_kernel<P, Q, T, VAR, 0, SC_CELLBUF>)
+                       : go(apply_fast_kernel<P, Q, T, VAR, 1, SC_CELLBUF>);
     } else {
       switch (stages) {
-        case 0: st = go(apply_fast_kernel<P, Q, T, VAR, 0, false>); break;
-        case 1: st = go(apply_fast_kernel<P, Q, T, VAR, 1, false>); break;
-        case 2: st = go(apply_fast_kernel<P, Q, T, VAR, 2, false>); break;
-        default: st = go(apply_fast_kernel<P, Q, T, VAR, 3, false>); break;
+        case 0: st = go(apply_fast_kernel<P, Q, T, VAR, 0, SC_ATOMIC>); break;
+        case 1: st = go(apply_fast_kernel<P, Q, T, VAR, 1, SC_ATOMIC>); break;
+        case 2: st = go(apply_fast_kernel<P, Q, T, VAR, 2, SC_ATOMIC>); break;
+        default: st = go(apply_fast_kernel<P, Q, T, VAR, 3, SC_ATOMIC>); break;
       }
     }
     if (st != LSMF_OK) return st;

@@ -428,8 +428,8 @@ static lsmf_status validate_params(const ProblemParams &P, int &caching) {
     set_error("MF level precision must be float or double");
     return LSMF_ERR_PRM;
   }
-  if (P.scatter != "atomic" && P.scatter != "colour8") {
-    set_error("MF scatter must be atomic or colour8");
+  if (P.scatter != "atomic" && P.scatter != "colour8" && P.scatter != "nodesum") {
+    set_error("MF scatter must be atomic, colour8 or nodesum");
     return LSMF_ERR_PRM;
   }
   if (P.type != "Cook" && P.type != "Box") {
@@ -506,9 +506,10 @@ lsmf_status lsmf_problem_create(const char *text, lsmf_problem **out) {
     gd.coarse_accurate_eig = P.coarse_accurate_eig;
     if ((s = lsmf_gmg_create(pb->mesh, &gd, &pb->gmg)) != LSMF_OK) { delete pb; return s; }
   }
-  if (P.scatter == "colour8") {
-    pb->op->scatter = LSMF_SCATTER_COLOUR8;
-    if (pb->gmg && (s = lsmf_gmg_set_option(pb->gmg, LSMF_GMG_OPT_SCATTER, LSMF_SCATTER_COLOUR8)) != LSMF_OK) {
+  if (P.scatter != "atomic") {
+    const int mode = P.scatter == "colour8" ? LSMF_SCATTER_COLOUR8 : LSMF_SCATTER_NODESUM;
+    if ((s = set_scatter_mode(pb->op, mode)) != LSMF_OK ||
+        (pb->gmg && (s = lsmf_gmg_set_option(pb->gmg, LSMF_GMG_OPT_SCATTER, mode)) != LSMF_OK)) {
       delete pb;
       return s;
     }

@@ -60,8 +60,8 @@ lsmf_status cheb_first_async(T *x, T *xold, const T *b, T *r, const T *invd, con
 template <typename T>
 lsmf_status cheb_step_async(T *x, T *xold, const T *b, T *r, const T *invd, const uint8_t *cmask, double f1, double f2,
                             bool has_old, size_t n, cudaStream_t st);
-// scatter: LSMF_SCATTER_ATOMIC, or LSMF_SCATTER_COLOUR8 (one launch per
-// colour of the coarse cells, plain adds, bit-reproducible)
+// scatter: LSMF_SCATTER_ATOMIC, or any other mode: one launch per colour
+// of the coarse cells, plain adds, bit-reproducible
 template <typename T>
 lsmf_status restrict_add_async(const Level &C, const TransferMap &TM, const T *b, const T *r, T *coarse, int scatter,
                                cudaStream_t st);
@@ -120,7 +120,7 @@ struct lsmf_gmg {
   // set-up (vstale) and applied to the executable graph in place when the
   // launch sequence is unchanged
   bool use_graph = true;
-  int scatter = LSMF_SCATTER_ATOMIC;  // cell loops and transfers: atomics or colour8
+  int scatter = LSMF_SCATTER_ATOMIC;  // LSMF_SCATTER_* of the level operators; transfers: atomics or colours
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t vexec = nullptr;
   bool vstale = true;

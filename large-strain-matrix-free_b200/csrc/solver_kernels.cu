@@ -921,7 +921,9 @@ static Prol1D<P> make_prol(const TransferMap &T) {
 // scatter once per lattice colour in the order 0..7 (plain adds).
 template <typename F>
 static lsmf_status over_colours(const Level &L, int scatter, F &&f) {
-  if (scatter == LSMF_SCATTER_COLOUR8) {
+  // colour8 and nodesum (whose node sums serve only the vmult) both run the
+  // deterministic colours here
+  if (scatter != LSMF_SCATTER_ATOMIC) {
     for (int c = 0; c < 8; ++c) {
       const int n = L.colour_off[c + 1] - L.colour_off[c];
       if (n > 0) LSMF_TRY(f(L.d_colour_cells.ptr + L.colour_off[c], n, 1));

@@ -20,7 +20,7 @@ LIB_PATH = os.path.join(HERE, "liblsmf.so")
 
 CACHING = {"scalar": 0, "tensor2": 1, "tensor4": 2, "scalar_referential": 3, "tensor4_ns": 4}
 GEOM = {"box": 0, "cook": 1}
-SCATTER = {"atomic": 0, "colour8": 1}
+SCATTER = {"atomic": 0, "colour8": 1, "nodesum": 2}
 MASK_ZERO, MASK_MPI, MASK_RW, MASK_SF, MASK_QD, MASK_DEFAULT = 1, 2, 4, 8, 16, 31
 
 
@@ -341,8 +341,9 @@ class NeoHookOperator:
         check(lib().lsmf_operator_set_option(self.h, 4, int(tries)))
 
     def set_scatter(self, mode):
-        """'atomic' (default) or 'colour8' (8 colour launches, plain adds:
-        bit-reproducible)."""
+        """'atomic' (default), 'colour8' (8 colour launches, plain adds:
+        bit-reproducible) or 'nodesum' (one cell loop into a per-cell buffer,
+        then per-node sums in cell order: bit-reproducible)."""
         check(lib().lsmf_operator_set_option(self.h, 5, SCATTER[mode] if isinstance(mode, str) else int(mode)))
 
     def set_record_prefetch(self, mode):

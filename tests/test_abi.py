@@ -58,6 +58,12 @@ def test_prm_every_caching(caching):
     assert st == 0, msg
 
 
+@pytest.mark.parametrize("scatter", ["atomic", "colour8", "nodesum"])
+def test_prm_every_scatter(scatter):
+    st, msg = lsmf.prm_validate(prm_text(dict(BASE, **{"MF scatter": scatter})))
+    assert st == 0, msg
+
+
 @pytest.mark.parametrize("change,status", [
     ({"Solver type": "CG"}, 10),                      # matrix-based path is not part of this library
     ({"Preconditioner type": "amg"}, 10),
@@ -71,6 +77,7 @@ def test_prm_every_caching(caching):
     ({"Dirichlet IDs and component mask": "2:true,true,true"}, 9),  # no mask for id 1
     ({"Preconditioner relaxation": "abc"}, 9),
     ({"Shear modulus": "-1"}, 9),
+    ({"MF scatter": "sometimes"}, 9),
 ])
 def test_prm_rejected(change, status):
     v = dict(BASE)
