@@ -559,6 +559,35 @@ def profile_vcycle(cells=15, refinements=1):
     return 0
 
 
+def profile_pairs(sizes=(48, 15)):
+    """One FP32 vmult per (cells^3 Q2 cube, tensor4 / tensor2, one cell per
+    warp / cell pairs), plain record loads, no warm-up: the launches that an
+    ncu capture of apply_fast_kernel and apply_pair_kernel compares."""
+    import torch
+    import lsmf
+    for n in sizes:
+        mesh = lsmf.Mesh("box", (n,) * 3, 0, degree=2)
+        mesh.set_dirichlet([(4, 7)])
+        nc, nn, nd = mesh.info()
+        X, _, _ = mesh.arrays()
+        mu = np.random.default_rng(1).choice([1.0, 10.0], nc)
+        u = torch.tensor(smooth_field(X, 3).reshape(-1), device="cuda").float()
+        src = torch.tensor(np.random.default_rng(2).uniform(-1, 1, nd), device="cuda").float()
+        for variant in ("tensor4", "tensor2"):
+            op = lsmf.NeoHookOperator(mesh, variant, 1, "fp32")
+            op.set_material(mu, NU)
+            op.cache(u)
+            op.set_pipeline(0)
+            for pairs in (0, 1):
+                op.set_cell_pairs(pairs)
+                dst = torch.empty_like(src)
+                op.vmult(dst, src)
+            torch.cuda.synchronize()
+            del op
+    print(json.dumps({"profile_pairs": "done", "sizes": list(sizes)}), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------- GPU (lsmf)
 def run_lsmf(args):
     import torch
@@ -839,6 +868,8 @@ def main():
                     help="only one FP32 V-cycle between cudaProfilerStart / Stop (for ncu --profile-from-start off)")
     ap.add_argument("--profile-cells", type=int, default=15, help="coarse cells per direction of --profile-vcycle")
     ap.add_argument("--profile-refinements", type=int, default=1, help="refinements of --profile-vcycle")
+    ap.add_argument("--profile-pairs", action="store_true",
+                    help="only one FP32 vmult per (48^3 / 15^3, tensor4 / tensor2, one cell / cell pairs) for ncu")
     ap.add_argument("--c5", action="store_true",
                     help="only the large configurations (128^3 Q2, 48^3 Q4 vmults; 128^3 inclusion Newton step)")
     args = ap.parse_args()
@@ -846,6 +877,8 @@ def main():
         return run_reference(args)
     if args.profile_vcycle:
         return profile_vcycle(args.profile_cells, args.profile_refinements)
+    if args.profile_pairs:
+        return profile_pairs()
     if args.c5:
         print(json.dumps(c5_measurements()), flush=True)
         return 0
