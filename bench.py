@@ -559,6 +559,36 @@ def profile_vcycle(cells=15, refinements=1):
     return 0
 
 
+def profile_setup(cells=15, refinements=2, precision="fp32"):
+    """One multigrid set-up (level caches, diagonals, Chebyshev eigenvalue
+    estimates, the coarse solver's accurate estimate) of the cells^3 ->
+    (cells 2^refinements)^3 Q2 tensor4 hierarchy, Chebyshev degree 4, between
+    cudaProfilerStart / Stop after one untimed set-up; prints its
+    event-timed duration."""
+    import torch
+    import lsmf
+    mesh = lsmf.Mesh("box", (cells,) * 3, refinements, degree=2)
+    mesh.set_dirichlet([(4, 7)])
+    nc, nn, nd = mesh.info()
+    X, _, _ = mesh.arrays()
+    u = torch.tensor(smooth_field(X, 1).reshape(-1), device="cuda")
+    g = lsmf.GMG(mesh, "tensor4", 1, precision, degree=4)
+    g.set_material(np.ones(nc), NU)
+    g.setup(u)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.profiler.start()
+    a.record(stream)
+    g.setup(u)
+    b.record(stream)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"profile_setup": "done", "ms": round(a.elapsed_time(b), 3),
+                      "levels": [g.level_info(l).tolist() for l in range(mesh.n_levels)]}), flush=True)
+    return 0
+
+
 def profile_pairs(sizes=(48, 15)):
     """One FP32 vmult per (cells^3 Q2 cube, tensor4 / tensor2, one cell per
     warp / cell pairs), plain record loads, no warm-up: the launches that an
@@ -868,6 +898,8 @@ def main():
                     help="only one FP32 V-cycle between cudaProfilerStart / Stop (for ncu --profile-from-start off)")
     ap.add_argument("--profile-cells", type=int, default=15, help="coarse cells per direction of --profile-vcycle")
     ap.add_argument("--profile-refinements", type=int, default=1, help="refinements of --profile-vcycle")
+    ap.add_argument("--profile-setup", action="store_true",
+                    help="only one FP32 multigrid set-up of the 15^3 -> 60^3 hierarchy between cudaProfilerStart / Stop")
     ap.add_argument("--profile-pairs", action="store_true",
                     help="only one FP32 vmult per (48^3 / 15^3, tensor4 / tensor2, one cell / cell pairs) for ncu")
     ap.add_argument("--c5", action="store_true",
@@ -879,6 +911,8 @@ def main():
         return profile_vcycle(args.profile_cells, args.profile_refinements)
     if args.profile_pairs:
         return profile_pairs()
+    if args.profile_setup:
+        return profile_setup()
     if args.c5:
         print(json.dumps(c5_measurements()), flush=True)
         return 0

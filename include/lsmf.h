@@ -231,9 +231,10 @@ lsmf_status lsmf_gmg_level_operator(lsmf_gmg *g, int level, lsmf_op **op);
  * captures the new launch sequence and updates the executable graph in
  * place, or instantiates it again when the sequence changed (another coarse
  * Chebyshev degree).  0 launches the kernels one by one.
- * LSMF_GMG_OPT_SCATTER: LSMF_SCATTER_ATOMIC (default) or
- * LSMF_SCATTER_COLOUR8 for every level operator, diagonal, restriction and
- * prolongation (a bit-reproducible V-cycle). */
+ * LSMF_GMG_OPT_SCATTER: LSMF_SCATTER_ATOMIC (default), LSMF_SCATTER_COLOUR8
+ * or LSMF_SCATTER_NODESUM for every level operator; diagonal, restriction
+ * and prolongation use the colours for either deterministic mode (a
+ * bit-reproducible V-cycle). */
 enum { LSMF_GMG_OPT_GRAPH = 1, LSMF_GMG_OPT_SCATTER = 2 };
 lsmf_status lsmf_gmg_set_option(lsmf_gmg *g, int option, int value);
 
