@@ -632,6 +632,10 @@ def run_lsmf(args):
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        # replicas: every rank runs the headline vmult and the end-to-end
+        # pass; the single-GPU diagnostics (variants, large meshes, Newton,
+        # adjoint) and the CPU baseline belong to the N = 1 run
+        args.no_variants = args.no_large = args.no_newton = args.no_adjoint = args.no_cpu = True
 
     seed = 1234
     assert min_det_f(seed) > 0.5
@@ -852,7 +856,7 @@ def run_lsmf(args):
         adjoint = adjoint_times()
 
     cpu = None
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         rate, t, _ = cpu_vmult_rate(args.cells, "tensor4", False, 5)
         cpu = {"value": rate, "unit": "GDoF/s", "cores": threads, "kind": "port",
