@@ -109,3 +109,29 @@ def test_partitioned_cg_with_poisoned_buffers():
     xg = xg.cpu().numpy()
     for p, x in zip(parts, xl):
         assert np.max(np.abs(x.cpu().numpy() - xg[p["gd"]])) <= 1e-9 * np.max(np.abs(xg))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("caching", ["tensor4", "tensor2"])
+def test_nodesum_vmult_with_poisoned_buffers(precision, caching):
+    # the per-cell buffer of the node-sum scatter is new device memory: every
+    # slot must be written by the cell loop before the node sums read it
+    gm = lsmf.Mesh("box", (3, 2, 3), 1, degree=2)
+    gm.set_dirichlet([(4, 7)])
+    nc, nn, nd = gm.info()
+    X, _, _ = gm.arrays()
+    rng = np.random.default_rng(9)
+    mu = rng.choice([1.0, 10.0], size=nc)
+    dt = torch.float64 if precision == "fp64" else torch.float32
+    u = torch.tensor((0.02 * np.sin(np.pi * X[:, [1, 2, 0]])).reshape(-1), device="cuda", dtype=dt)
+    src = torch.tensor(rng.uniform(-1, 1, nd), device="cuda", dtype=dt)
+    op = lsmf.NeoHookOperator(gm, caching, 1, precision)
+    op.set_material(mu, 0.3)
+    op.cache(u)
+    a = torch.empty_like(src)
+    op.vmult(a, src)
+    op.set_scatter("nodesum")
+    b = torch.empty_like(src)
+    op.vmult(b, src)
+    assert torch.all(torch.isfinite(b))
+    assert (torch.max(torch.abs(a - b)) / torch.max(torch.abs(a))).item() < (1e-13 if precision == "fp64" else 2e-6)
