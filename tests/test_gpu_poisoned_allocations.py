@@ -10,7 +10,8 @@ held a NaN or an infinity was handed back.
 
 Covered: CG with no, Jacobi and GMG preconditioning; a Newton solve and the
 adjoint gradient of both formulations against the oracle; the partitioned
-(two-part) Jacobi CG against the whole-mesh CG.
+(two-part) Jacobi CG against the whole-mesh CG; the node-sum vmult (its
+per-cell buffer) against the atomic one.
 """
 import numpy as np
 import pytest

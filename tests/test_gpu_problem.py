@@ -14,8 +14,8 @@
    modulus against central finite differences (20 seeded directions, step
    1e-6) within 1e-6, and entrywise against the oracle's FP64 reference
    gradient (its own adjoint solve with tau differentiated in mu) within
-   1e-8, formulations 0 and 1; the same FD check on the 32^3 Q2 benchmark
-   mesh (823,875 DoFs).
+   1e-8, formulations 0 and 1; the same FD check on the benchmark's voids
+   mesh (8^3 coarse cells minus 16 spheres, refined twice: 808,587 DoFs).
 """
 import json
 import os
@@ -201,18 +201,22 @@ def test_adjoint_gradient_matches_oracle_gradient(formulation, parity):
 
 
 def test_adjoint_config_size_finite_differences(parity):
-    """The adjoint benchmark workload (32^3 Q2 cube, 823,875 DoFs, log mu ~
-    N(0, 0.3^2), top-face misfit): 20 seeded +-1 directions (each cell's
-    log mu moves by the step 1e-6), max |fd - g.v| <= 1e-6 max |fd|."""
+    """The adjoint benchmark workload (the voids mesh reduced to ~1 M DoFs:
+    8^3 coarse cells minus the 16 seeded spheres, refined twice, 808,587
+    DoFs; log mu ~ N(0, 0.3^2), top-face misfit): 20 seeded +-1 directions
+    (each cell's log mu moves by the step 1e-6), max |fd - g.v| <= 1e-6
+    max |fd|."""
     import bench
     pb = lsmf.Problem(bench.adjoint_prm())
-    assert pb.n_dofs == 823875
+    om = O.Mesh(O.GEOM_BOX, (8, 8, 8), 2, (0, 0, 0), (1, 1, 1), 1.0, 2, 3,
+                coarse_active=O.void_mask((8, 8, 8), 16, 0.08, 2024))
+    assert (pb.n_cells, pb.n_dofs) == (om.n_cells, om.n_dofs) == (31872, 808587)
     rng = np.random.default_rng(4321)
     theta = rng.normal(0.0, 0.3, pb.n_cells)
     target = rng.uniform(-1e-3, 1e-3, pb.n_dofs)
     pb.adjoint_forward(theta, target, 5)
     grad = pb.adjoint_backward()
     fd, ad = bench.fd_check(pb, theta, target, grad, rng, 20, 1e-6)
-    parity("adjoint vs central FD, 32^3 Q2 (823,875 DoFs), 20 directions, h = 1e-6",
+    parity("adjoint vs central FD, voids 32^3 Q2 (808,587 DoFs), 20 directions, h = 1e-6",
            np.max(np.abs(fd - ad)) / np.max(np.abs(fd)), 1e-6)
     assert np.max(np.abs(fd - ad)) <= 1e-6 * np.max(np.abs(fd)), (fd, ad)
