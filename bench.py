@@ -477,28 +477,42 @@ def vmult_rate(cells, degree, variant, prec, reps=10, seed=77):
             "frac_hbm": round(by / (ms * 1e-3) / 1e9 / peak, 3)}
 
 
-def inclusions_prm(level_precision, cells=16, refinements=3):
-    """128^3 Q2 unit cube (50,923,779 DoFs): bottom clamped, top displaced
-    by -0.01 in z (first of 10 load steps), FP64 outer CG to 1e-8, Chebyshev
-    degree 4 smoother on FP32 or FP64 levels; mu is set per cell afterwards."""
+def inclusions_prm(level_precision, cells=16, refinements=3, fe_degree=2):
+    """128^3 Q2 unit cube (50,923,779 DoFs; fe_degree 4 with 12^3 coarse
+    cells refined twice: 48^3 Q4, 21,567,171 DoFs): bottom clamped, top
+    displaced by -0.01 in z (first of 10 load steps), FP64 outer CG to 1e-8,
+    Chebyshev degree 4 smoother on FP32 or FP64 levels of the same element
+    degree; mu is set per cell afterwards."""
     return voids_prm(level_precision, cells, refinements).replace(
-        "  set Void spheres = 16, 0.08, 2024\n", "")
+        "  set Void spheres = 16, 0.08, 2024\n", "").replace(
+        "  set Polynomial degree = 2", "  set Polynomial degree = %d" % fe_degree).replace(
+        "  set Quadrature order = 3", "  set Quadrature order = %d" % (fe_degree + 1))
 
 
 def inclusion_mu(coarse=16, refinements=3, seed=99, n_spheres=32, target_fraction=0.2):
-    """mu = 10 in seeded spheres (about 20 % of the volume), 1 elsewhere, per
-    fine cell of the structured unit cube (cell centres), in the cell order
-    of the problem's mesh (the same coarse cells and refinements)."""
+    """mu = 10 in seeded spheres covering 20 % of the volume, 1 elsewhere,
+    per fine cell of the structured unit cube (cell centres), in the cell
+    order of the problem's mesh (the same coarse cells and refinements).  The
+    common radius is found by bisection so that the covered fraction of the
+    cells (overlaps and the parts outside the cube do not count) reaches the
+    target."""
     import lsmf
     rng = np.random.default_rng(seed)
-    r = (target_fraction * 3.0 / (4.0 * np.pi * n_spheres)) ** (1.0 / 3.0)
     centres = rng.uniform(0, 1, (n_spheres, 3))
     mesh = lsmf.Mesh("box", (coarse,) * 3, refinements, degree=1)
     _, _, ijk = mesh.arrays()
     xc = (ijk + 0.5) / (coarse << refinements)
-    inside = np.zeros(len(xc), dtype=bool)
+    d2 = np.full(len(xc), np.inf)
     for c in centres:
-        inside |= np.sum((xc - c) ** 2, axis=1) <= r * r
+        np.minimum(d2, np.sum((xc - c) ** 2, axis=1), out=d2)
+    lo, hi = 0.0, 1.0
+    for _ in range(60):
+        r = 0.5 * (lo + hi)
+        if np.mean(d2 <= r * r) < target_fraction:
+            lo = r
+        else:
+            hi = r
+    inside = d2 <= hi * hi
     return np.where(inside, 10.0, 1.0), float(inside.mean())
 
 
@@ -510,10 +524,17 @@ def c5_measurements(repeats=3):
     for cells, degree in ((128, 2), (48, 4)):
         for prec in ("fp64", "fp32"):
             out["vmult"]["%d^3_Q%d_tensor4_%s" % (cells, degree, prec)] = vmult_rate(cells, degree, "tensor4", prec)
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
     mu, frac = inclusion_mu()
-    out.update(compare_level_precisions(inclusions_prm, repeats, int(os.environ.get("LOCAL_RANK", "0")), mu))
+    out.update(compare_level_precisions(inclusions_prm, repeats, dev, mu))
     out["workload"] = ("inclusions: 128^3 Q2 unit cube, mu = 10 in 32 seeded spheres (%.1f %% of the cells), "
                        "tensor4, first load step, CG to 1e-8" % (100 * frac))
+    # the same inclusion field on 48^3 Q4 cells (Q4 multigrid levels 12^3, 24^3, 48^3)
+    mu4, frac4 = inclusion_mu(coarse=12, refinements=2)
+    q4 = compare_level_precisions(lambda prec: inclusions_prm(prec, 12, 2, fe_degree=4), repeats, dev, mu4)
+    q4["workload"] = ("inclusions: 48^3 Q4 unit cube, mu = 10 in 32 seeded spheres (%.1f %% of the cells), "
+                      "tensor4, first load step, CG to 1e-8" % (100 * frac4))
+    out["q4_newton"] = q4
     return out
 
 

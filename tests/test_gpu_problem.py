@@ -90,6 +90,30 @@ def test_newton_gmg_matches_oracle(precision, parity):
     assert np.max(np.abs(u - ref["u"])) <= U_TOL * np.max(np.abs(ref["u"]))
 
 
+@pytest.mark.parametrize("precision", ["float", "double"])
+def test_newton_gmg_q4_matches_oracle(precision, parity):
+    # Q4 elements (5^3 Gauss points) with Q4 multigrid levels
+    prm = prm_text(dict({
+        "Polynomial degree": 4, "Quadrature order": 5, "Dimension": 3, "Type": "Box", "Box cells": "1, 1, 1",
+        "Global refinement": 2, "Poisson's ratio": 0.3, "Shear modulus": 1.0, "Formulation": 1,
+        "Solver type": "MF_CG", "Preconditioner type": "gmg", "MF caching": "tensor4",
+        "MF level precision": precision, "Dirichlet IDs and expressions": "4:0,0,0",
+        "Dirichlet IDs and component mask": "4:true,true,true",
+        "Neumann IDs and expressions": "5:0.02*t,0,-0.05*t", "End time": 1, "Time step size": 0.5}, **TIGHT))
+    pb = lsmf.Problem(prm)
+    res = pb.run()
+    ref = O.newton(geometry=O.GEOM_BOX, coarse=(1, 1, 1), n_refinements=2, p=4, q=5, caching="tensor4",
+                   formulation=1, mu=1.0, nu=0.3, dirichlet=[(4, 7, (0, 0, 0))],
+                   neumann=[(5, (0, 0, 0), (0.02, 0, -0.05))], end_time=1.0, dt=0.5, precond="gmg",
+                   level_fp32=(precision == "float"), return_u=True, **TIGHT_ORACLE)
+    assert ref["rc"] == 0
+    assert [s["newton_iterations"] for s in res["steps"]] == [s["newton_iterations"] for s in ref["steps"]]
+    u = pb.solution()
+    parity("Q4 box GMG Newton (%s levels): displacement" % precision,
+           np.max(np.abs(u - ref["u"])) / np.max(np.abs(ref["u"])), U_TOL)
+    assert np.max(np.abs(u - ref["u"])) <= U_TOL * np.max(np.abs(ref["u"]))
+
+
 def test_newton_gmg_gc_equals_gmg():
     # global coarsening on a globally refined mesh builds the same levels and
     # transfers, so the solve is the same

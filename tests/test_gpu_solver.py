@@ -110,6 +110,33 @@ def test_vcycle_graph_follows_each_setup(precision):
         assert np.max(np.abs(ddst.cpu().numpy() - want)) <= tol * np.max(np.abs(want)), scale
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("p", [1, 3, 4])
+def test_vcycle_other_degrees_match_oracle(precision, p):
+    # h-multigrid with Q_p on every level (the transfer maps of degree p, the
+    # level operators' sweeps of degree p)
+    coarse, nref = ((2, 2, 2), 2) if p == 1 else ((1, 1, 1), 2)
+    gm, mu, u, dirichlet, (lo, hi), rng = _problem("tensor4", 1, p=p, coarse=coarse, nref=nref)
+    og = O.GMG(O.GEOM_BOX, coarse, nref, lo, hi, 1.0, p, p + 1, "tensor4", 1, precision == "fp32", mu, 0.3,
+               dirichlet, u)
+    g = lsmf.GMG(gm, "tensor4", 1, precision)
+    g.set_material(mu, 0.3)
+    g.setup(torch.tensor(u, device="cuda"))
+    tol = 1e-9 if precision == "fp64" else 2e-3
+    for l in range(gm.n_levels):
+        a, b = g.level_info(l), og.level_info(l)
+        assert a[2] == b[2], (l, a, b)
+        assert abs(a[0] - b[0]) <= tol * abs(b[1]) and abs(a[1] - b[1]) <= tol * abs(b[1]), (l, a, b)
+    src = rng.uniform(-1, 1, u.size)
+    src[gm.constraint_mask() == 1] = 0
+    dsrc = torch.tensor(src, device="cuda")
+    ddst = torch.empty_like(dsrc)
+    g.vmult(ddst, dsrc)
+    want = og.vmult(src)
+    vtol = 1e-10 if precision == "fp64" else 1e-4
+    assert np.max(np.abs(ddst.cpu().numpy() - want)) <= vtol * np.max(np.abs(want))
+
+
 def test_vcycle_cook_geometry():
     gm, mu, u, dirichlet, (lo, hi), rng = _problem("tensor4", 1, coarse=(2, 2, 1), nref=1, geometry="cook")
     og = O.GMG(O.GEOM_COOK, (2, 2, 1), 1, lo, hi, 1.0, 2, 3, "tensor4", 1, False, mu, 0.3, dirichlet, u)
