@@ -94,9 +94,10 @@ template <typename T>
 __device__ __forceinline__ void atomic_add(T *a, T v) { atomicAdd(a, v); }
 
 // ------------------------------------------------ bulk-copy (TMA) helpers
-// One-dimensional cp.async.bulk global -> shared with mbarrier completion
-// (no tensor map, no multicast): each cell record is one contiguous,
-// 16-byte aligned block of ncomp * Q^3 values.
+// One-dimensional cp.async.bulk from this GPU's global memory into the
+// issuing CTA's own shared memory with mbarrier completion (no tensor map):
+// each cell record is one contiguous, 16-byte aligned block of
+// ncomp * Q^3 values.
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
