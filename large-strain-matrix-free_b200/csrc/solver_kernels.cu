@@ -412,57 +412,73 @@ __global__ void cheb_step_kernel(T *__restrict__ x, T *__restrict__ xold, const 
 }
 
 // ------------------------------------------------------------------ transfer
-template <int P>
+// 1D prolongation matrix in the level's arithmetic type (FP32 levels add in
+// FP32, FP64 levels in FP64)
+template <int P, typename C>
 struct Prol1D {
-  double m[2 * P + 1][P + 1];
+  C m[2 * P + 1][P + 1];
 };
 
 // one warp per coarse cell.  restriction: coarse += R (weight * (b - r))
 // on the fine level, coarse Dirichlet entries dropped (restrict_and_add).
 // cells / plain: the coarse cells of one lattice colour (no two share a
 // node) with plain adds, or (cells == nullptr) all n_coarse cells with
-// atomics.
+// atomics.  Every load that depends only on the coarse cell (its fine
+// block's node ids, its own node ids) is issued first, then every load that
+// depends on those (weights, fine values), so a cell costs two round trips.
 template <int P, typename T>
 __global__ void restrict_kernel(int n_coarse, const int *__restrict__ cells, int plain, const int *__restrict__ coarse_cn,
                                 const int *__restrict__ fine_nodes, const double *__restrict__ weight,
-                                const T *__restrict__ b, const T *__restrict__ r, T *coarse, Prol1D<P> pm) {
+                                const T *__restrict__ b, const T *__restrict__ r, T *coarse, Prol1D<P, T> pm) {
   constexpr int N1 = P + 1, NF = 2 * P + 1, NFB = NF * NF * NF, NCN = N1 * N1 * N1;
   constexpr int SZ = 3 * NFB + 3 * NF * NF * N1 + 3 * NF * N1 * N1;
+  constexpr int NPL = (NFB + 31) / 32, CPL = (3 * NCN + 31) / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-  double *in = (double *)smem_raw + warp * SZ, *s1 = in + 3 * NFB, *s2 = s1 + 3 * NF * NF * N1;
+  T *in = (T *)smem_raw + warp * SZ, *s1 = in + 3 * NFB, *s2 = s1 + 3 * NF * NF * N1;
   for (int ic = blockIdx.x * wpb + warp; ic < n_coarse; ic += gridDim.x * wpb) {
     const int c = cells ? __ldg(cells + ic) : ic;
     const int *fn = fine_nodes + (size_t)c * NFB;
-    // gather the fine block: all node ids of the lane first, then all
-    // weights and values, so every load of the lane is in flight at once
-    constexpr int NPL = (NFB + 31) / 32;
-    int node[NPL];
+    int node[NPL], cpk[CPL];
 #pragma unroll
     for (int q = 0; q < NPL; ++q) node[q] = (lane + 32 * q < NFB) ? __ldg(fn + lane + 32 * q) : -1;
-    double w[NPL], bv[NPL][3], rv[NPL][3];
 #pragma unroll
-    for (int q = 0; q < NPL; ++q) {
-      if (node[q] < 0) continue;
-      w[q] = __ldg(weight + node[q]);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const size_t d = 3 * (size_t)node[q] + k;
-        bv[q][k] = (double)b[d];
-        rv[q][k] = r ? (double)r[d] : 0.0;
-      }
+    for (int q = 0; q < CPL; ++q) {
+      const int it = lane + 32 * q;
+      cpk[q] = it < 3 * NCN ? __ldg(coarse_cn + (size_t)c * NCN + it % NCN) : 0;
     }
+    // weights and values in chunks of CH fine nodes per lane (all of them
+    // at degree <= 2; degree 3 / 4 blocks of 343 / 729 nodes would otherwise
+    // hold 7 values x 11 / 23 nodes per lane in registers)
+    constexpr int CH = NPL < 4 ? NPL : 4;
 #pragma unroll
-    for (int q = 0; q < NPL; ++q) {
-      if (node[q] < 0) continue;
+    for (int q0 = 0; q0 < NPL; q0 += CH) {
+      T w[CH], bv[CH][3], rv[CH][3];
 #pragma unroll
-      for (int k = 0; k < 3; ++k) in[k * NFB + lane + 32 * q] = w[q] * (bv[q][k] - rv[q][k]);
+      for (int j = 0; j < CH; ++j) {
+        const int q = q0 + j;
+        if (q >= NPL || node[q] < 0) continue;
+        w[j] = T(__ldg(weight + node[q]));
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const size_t d = 3 * (size_t)node[q] + k;
+          bv[j][k] = b[d];
+          rv[j][k] = r ? r[d] : T(0);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < CH; ++j) {
+        const int q = q0 + j;
+        if (q >= NPL || node[q] < 0) continue;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) in[k * NFB + lane + 32 * q] = w[j] * (bv[j][k] - rv[j][k]);
+      }
     }
     __syncwarp();
     // z: s1[k][z][fy][fx] = sum_fz P[fz][z] in[k][fz][fy][fx]
     for (int it = lane; it < 3 * N1 * NF * NF; it += 32) {
       const int fyx = it % (NF * NF), z = (it / (NF * NF)) % N1, k = it / (NF * NF * N1);
-      double s = 0;
+      T s = 0;
 #pragma unroll
       for (int fz = 0; fz < NF; ++fz) s += pm.m[fz][z] * in[k * NFB + fz * NF * NF + fyx];
       s1[it] = s;
@@ -471,60 +487,75 @@ __global__ void restrict_kernel(int n_coarse, const int *__restrict__ cells, int
     // y: s2[k][z][y][fx]
     for (int it = lane; it < 3 * N1 * N1 * NF; it += 32) {
       const int fx = it % NF, y = (it / NF) % N1, kz = it / (NF * N1);
-      double s = 0;
+      T s = 0;
 #pragma unroll
       for (int fy = 0; fy < NF; ++fy) s += pm.m[fy][y] * s1[(kz * NF + fy) * NF + fx];
       s2[it] = s;
     }
     __syncwarp();
     // x: coarse value of node (x, y, z)
-    for (int it = lane; it < 3 * NCN; it += 32) {
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) {
+      const int it = lane + 32 * q;
+      if (it >= 3 * NCN) continue;
       const int a = it % NCN, k = it / NCN, x = a % N1, zy = a / N1;
-      double s = 0;
+      T s = 0;
 #pragma unroll
       for (int fx = 0; fx < NF; ++fx) s += pm.m[fx][x] * s2[zy * NF + fx + k * N1 * N1 * NF];
-      const int packed = coarse_cn[(size_t)c * NCN + a];
+      const int packed = cpk[q];
       if (!((packed >> (NODE_BITS + k)) & 1)) {
         T *dst = coarse + 3 * (size_t)(packed & NODE_MASK) + k;
-        if (plain) *dst += T(s);
-        else atomicAdd(dst, T(s));
+        if (plain) *dst += s;
+        else atomicAdd(dst, s);
       }
     }
     __syncwarp();
   }
 }
 
-// prolongation: fine += P coarse (coarse Dirichlet entries read as zero)
+// prolongation: fine += weight * P coarse (coarse Dirichlet entries read as
+// zero); the same two-round-trip load order as the restriction
 template <int P, typename T>
 __global__ void prolongate_kernel(int n_coarse, const int *__restrict__ cells, int plain,
                                   const int *__restrict__ coarse_cn, const int *__restrict__ fine_nodes,
-                                  const double *__restrict__ weight, const T *__restrict__ coarse, T *fine, Prol1D<P> pm) {
+                                  const double *__restrict__ weight, const T *__restrict__ coarse, T *fine,
+                                  Prol1D<P, T> pm) {
   constexpr int N1 = P + 1, NF = 2 * P + 1, NFB = NF * NF * NF, NCN = N1 * N1 * N1;
   constexpr int SZ = 3 * NCN + 3 * N1 * N1 * NF + 3 * N1 * NF * NF;
+  constexpr int NPL = (NFB + 31) / 32, CPL = (3 * NCN + 31) / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-  double *v = (double *)smem_raw + warp * SZ, *s1 = v + 3 * NCN, *s2 = s1 + 3 * N1 * N1 * NF;
-  constexpr int NPL = (NFB + 31) / 32;
+  T *v = (T *)smem_raw + warp * SZ, *s1 = v + 3 * NCN, *s2 = s1 + 3 * N1 * N1 * NF;
   for (int ic = blockIdx.x * wpb + warp; ic < n_coarse; ic += gridDim.x * wpb) {
     const int c = cells ? __ldg(cells + ic) : ic;
-    // the lane's fine nodes and weights, loaded before the sweeps
     const int *fn = fine_nodes + (size_t)c * NFB;
-    int node[NPL];
-    double w[NPL];
+    int node[NPL], cpk[CPL];
 #pragma unroll
     for (int q = 0; q < NPL; ++q) node[q] = (lane + 32 * q < NFB) ? __ldg(fn + lane + 32 * q) : -1;
 #pragma unroll
-    for (int q = 0; q < NPL; ++q) w[q] = node[q] >= 0 ? __ldg(weight + node[q]) : 0.0;
-    for (int it = lane; it < 3 * NCN; it += 32) {
-      const int a = it % NCN, k = it / NCN;
-      const int packed = coarse_cn[(size_t)c * NCN + a];
-      v[it] = ((packed >> (NODE_BITS + k)) & 1) ? 0.0 : (double)coarse[3 * (size_t)(packed & NODE_MASK) + k];
+    for (int q = 0; q < CPL; ++q) {
+      const int it = lane + 32 * q;
+      cpk[q] = it < 3 * NCN ? __ldg(coarse_cn + (size_t)c * NCN + it % NCN) : 0;
+    }
+    T w[NPL], cv[CPL];
+#pragma unroll
+    for (int q = 0; q < NPL; ++q) w[q] = node[q] >= 0 ? T(__ldg(weight + node[q])) : T(0);
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) {
+      const int it = lane + 32 * q, k = it / NCN;
+      cv[q] = (it < 3 * NCN && !((cpk[q] >> (NODE_BITS + k)) & 1))
+                  ? coarse[3 * (size_t)(cpk[q] & NODE_MASK) + k] : T(0);
+    }
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) {
+      const int it = lane + 32 * q;
+      if (it < 3 * NCN) v[it] = cv[q];
     }
     __syncwarp();
     // x: s1[k][z][y][fx]
     for (int it = lane; it < 3 * N1 * N1 * NF; it += 32) {
       const int fx = it % NF, zy = it / NF;  // zy = (k*N1 + z)*N1 + y
-      double s = 0;
+      T s = 0;
 #pragma unroll
       for (int x = 0; x < N1; ++x) s += pm.m[fx][x] * v[zy * N1 + x];
       s1[it] = s;
@@ -533,7 +564,7 @@ __global__ void prolongate_kernel(int n_coarse, const int *__restrict__ cells, i
     // y: s2[k][z][fy][fx]
     for (int it = lane; it < 3 * N1 * NF * NF; it += 32) {
       const int fx = it % NF, fy = (it / NF) % NF, kz = it / (NF * NF);
-      double s = 0;
+      T s = 0;
 #pragma unroll
       for (int y = 0; y < N1; ++y) s += pm.m[fy][y] * s1[(kz * N1 + y) * NF + fx];
       s2[it] = s;
@@ -545,12 +576,12 @@ __global__ void prolongate_kernel(int n_coarse, const int *__restrict__ cells, i
       const int l = lane + 32 * q, fyx = l % (NF * NF), fz = l / (NF * NF);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        double s = 0;
+        T s = 0;
 #pragma unroll
         for (int z = 0; z < N1; ++z) s += pm.m[fz][z] * s2[(k * N1 + z) * NF * NF + fyx];
         T *dst = fine + 3 * (size_t)node[q] + k;
-        if (plain) *dst += T(w[q] * s);
-        else atomicAdd(dst, T(w[q] * s));
+        if (plain) *dst += w[q] * s;
+        else atomicAdd(dst, w[q] * s);
       }
     }
     __syncwarp();
@@ -909,11 +940,11 @@ template lsmf_status cheb_step_async<float>(float *, float *, const float *, flo
 template lsmf_status cheb_step_async<double>(double *, double *, const double *, double *, const double *,
                                              const uint8_t *, double, double, bool, size_t, cudaStream_t);
 
-template <int P>
-static Prol1D<P> make_prol(const TransferMap &T) {
-  Prol1D<P> pm;
+template <int P, typename C>
+static Prol1D<P, C> make_prol(const TransferMap &T) {
+  Prol1D<P, C> pm;
   for (int f = 0; f < 2 * P + 1; ++f)
-    for (int x = 0; x <= P; ++x) pm.m[f][x] = T.P1[f * (P + 1) + x];
+    for (int x = 0; x <= P; ++x) pm.m[f][x] = C(T.P1[f * (P + 1) + x]);
   return pm;
 }
 
@@ -938,10 +969,10 @@ static lsmf_status transfer_impl(bool restrict_dir, const Level &C, const Transf
                                  T *coarse_or_fine, const T *coarse_src, int scatter, cudaStream_t st) {
   constexpr int N1 = P + 1, NF = 2 * P + 1;
   const int wpb = 4;
-  const Prol1D<P> pm = make_prol<P>(TM);
+  const Prol1D<P, T> pm = make_prol<P, T>(TM);
   if (restrict_dir) {
     constexpr int SZ = 3 * NF * NF * NF + 3 * NF * NF * N1 + 3 * NF * N1 * N1;
-    const size_t smem = sizeof(double) * SZ * wpb;
+    const size_t smem = sizeof(T) * SZ * wpb;
     auto k = restrict_kernel<P, T>;
     LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     LSMF_TRY(over_colours(C, scatter, [&](const int *cells, int n, int plain) -> lsmf_status {
@@ -953,7 +984,7 @@ static lsmf_status transfer_impl(bool restrict_dir, const Level &C, const Transf
     }));
   } else {
     constexpr int SZ = 3 * N1 * N1 * N1 + 3 * N1 * N1 * NF + 3 * N1 * NF * NF;
-    const size_t smem = sizeof(double) * SZ * wpb;
+    const size_t smem = sizeof(T) * SZ * wpb;
     auto k = prolongate_kernel<P, T>;
     LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     LSMF_TRY(over_colours(C, scatter, [&](const int *cells, int n, int plain) -> lsmf_status {
