@@ -85,3 +85,20 @@ def test_option_validation_and_fp64():
     a = _vmult(op, src)
     op.set_cell_pairs(1)   # FP64: ignored
     assert torch.equal(a, _vmult(op, src))
+
+
+@pytest.mark.parametrize("caching,formulation", VARIANTS)
+@pytest.mark.parametrize("p", [1, 2, 4])
+def test_single_cell_mesh(caching, formulation, p):
+    # one cell: the only pair has no partner (pairs) and every node belongs
+    # to exactly one cell (node sums)
+    gm, om, cmask, mu, u, src = _setup(p=p, coarse=(1, 1, 1), level=0)
+    op = _op(gm, mu, u, caching, formulation)
+    ref = _oracle_op(om, cmask, mu, u, caching, formulation)
+    want = ref.vmult(src)
+    for pairs in (0, 1):
+        op.set_cell_pairs(pairs)
+        for scatter in ("atomic", "colour8", "nodesum"):
+            op.set_scatter(scatter)
+            got = _vmult(op, src).double().cpu().numpy()
+            assert _rel(got, want) < 2e-5, (pairs, scatter)
