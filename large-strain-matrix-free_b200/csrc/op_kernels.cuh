@@ -1120,7 +1120,13 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
   // a warp's next cell: plain loads (15^3-cell FP64 coarse Chebyshev solve
   // 10.9 -> 9.9 ms per V-cycle, FP32 unchanged)
   if (op->stages < 0 && a.n_cells <= 32 * num_sms()) stages = 0;
-  const int max_warps = op->max_warps > 0 ? op->max_warps : ((VAR == VAR_TENSOR2 && sizeof(T) == 8) ? 8 : 4);
+  // 8 warps per block for the FP64 tensor2 and scalar kernels, 4 otherwise
+  // (measured at 64^3 Q2: scalar FP64 0.478 -> 0.466 ms, formulation 0
+  // 0.497 -> 0.482 ms)
+  const int max_warps =
+      op->max_warps > 0
+          ? op->max_warps
+          : (((VAR == VAR_TENSOR2 || VAR == VAR_SCALAR_F1 || VAR == VAR_SCALAR_F0) && sizeof(T) == 8) ? 8 : 4);
   if (rec_bytes % 16 != 0) stages = 0;
   // fewer stages when the ring would leave fewer than 4 warps per block
   while (stages > 0 && warps_for_budget(wbytes(stages), 8, 220 * 1024) < 4) --stages;
