@@ -144,7 +144,8 @@ lsmf_status lsmf_operator_el(lsmf_op *op, int row, int col, double *value);
  * LSMF_OPT_BASIC_KERNEL: 1 = the basic vmult kernel (per-warp shared-memory
  *   sweeps, plain loads); the stage mask of vmult always uses it.
  * LSMF_OPT_MAX_WARPS: cap on warps per block of the vmult kernel (1..8;
- *   0 = default: 8 for FP64 tensor2 and scalar, 4 otherwise).
+ *   0 = default: 8 for FP64 tensor2 and scalar, 2 for FP64
+ *   scalar_referential, 4 otherwise).
  * LSMF_OPT_WAIT_TRIES: bound of the pipelined kernel's wait for a cell
  *   record (mbarrier try_wait calls; -1 = default 2^22, seconds).  A wait
  *   that runs out sets the operator's device error word, lets every copy

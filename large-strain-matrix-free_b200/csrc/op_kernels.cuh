@@ -1120,13 +1120,17 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
   // a warp's next cell: plain loads (15^3-cell FP64 coarse Chebyshev solve
   // 10.9 -> 9.9 ms per V-cycle, FP32 unchanged)
   if (op->stages < 0 && a.n_cells <= 32 * num_sms()) stages = 0;
-  // 8 warps per block for the FP64 tensor2 and scalar kernels, 4 otherwise
-  // (measured at 64^3 Q2: scalar FP64 0.478 -> 0.466 ms, formulation 0
-  // 0.497 -> 0.482 ms)
+  // warps per block, swept 2 / 4 / 8 for every variant and precision at
+  // 64^3 Q2: 8 for the FP64 tensor2 and scalar kernels (scalar 0.478 ->
+  // 0.466 ms, formulation 0 0.497 -> 0.482 ms), 2 for FP64
+  // scalar_referential (0.467 -> 0.452 ms), 4 otherwise (the others within
+  // 1 % of each other)
+  constexpr bool fp64 = sizeof(T) == 8;
   const int max_warps =
-      op->max_warps > 0
-          ? op->max_warps
-          : (((VAR == VAR_TENSOR2 || VAR == VAR_SCALAR_F1 || VAR == VAR_SCALAR_F0) && sizeof(T) == 8) ? 8 : 4);
+      op->max_warps > 0 ? op->max_warps
+      : (fp64 && (VAR == VAR_TENSOR2 || VAR == VAR_SCALAR_F1 || VAR == VAR_SCALAR_F0)) ? 8
+      : (fp64 && VAR == VAR_SCALAR_REF) ? 2
+                                        : 4;
   if (rec_bytes % 16 != 0) stages = 0;
   // fewer stages when the ring would leave fewer than 4 warps per block
   while (stages > 0 && warps_for_budget(wbytes(stages), 8, 220 * 1024) < 4) --stages;
