@@ -191,3 +191,21 @@ def test_detf_nonpositive_reported():
     with pytest.raises(lsmf.LsmfError) as e:
         op.vmult(torch.empty_like(dsrc), dsrc)
     assert e.value.status == 4
+
+
+def test_cached_volume_ratio_matches_det_f():
+    """The reference's consistency check of the formulation-0 cache
+    (mf_nh_operator.h:1131-1156): at every point JxW_ref / JxW_cur * det F
+    = 1, with det F = c^-3 from the cached c = J^(-1/3).  On the box mesh the
+    reference JxW is h^3 times the Gauss weight of the point."""
+    gm, om, cmask, mu, u, src = _setup(p=2, coarse=(2, 2, 2), level=1)
+    op = lsmf.NeoHookOperator(gm, "scalar", 0, "fp64")
+    op.set_material(mu, 0.3)
+    op.cache(torch.tensor(u, device="cuda"))
+    c = op.table(0).reshape(-1, 27)
+    jxw = op.table(5).reshape(-1, 27)
+    g = np.array([5.0, 8.0, 5.0]) / 18.0  # 3-point Gauss weights on [0, 1]
+    wq = (g[None, None, :] * g[None, :, None] * g[:, None, None]).reshape(-1)  # q = qx + 3 qy + 9 qz
+    h = 0.25
+    ratio = (h ** 3 * wq[None, :]) / jxw * c ** -3.0
+    assert np.max(np.abs(ratio - 1.0)) < 1e-12

@@ -182,3 +182,22 @@ def test_matrix_based_tangent_equals_matrix_free_operator(formulation, caching):
     b = np.where(cm == 1, 0.0, rng.uniform(-1, 1, m.n_dofs))
     xk, itk, ok = O.cg_jacobi(K, b, 1e-10 * np.linalg.norm(b), 5000)
     assert ok and np.linalg.norm(op.vmult(xk) - b) <= 1.01e-10 * np.linalg.norm(b)
+
+
+def test_oracle_cached_volume_ratio_matches_det_f():
+    """The reference's consistency check of the formulation-0 cache
+    (mf_nh_operator.h:1131-1156) on the oracle: JxW_ref / JxW_cur * det F = 1
+    at every point, det F = c^-3 from the cached c = J^(-1/3), JxW_ref = h^3
+    times the Gauss weight on the box mesh."""
+    m = O.Mesh(O.GEOM_BOX, (2, 2, 2), 1, (0, 0, 0), (1, 1, 1), 1.0, 2, 3)
+    rng = np.random.default_rng(4)
+    op = O.Operator(m, "scalar", 0)
+    op.set_material(rng.choice([1.0, 10.0], m.n_cells), 0.3)
+    op.set_constraints(m.constraints([(4, 7)]))
+    assert op.cache(rng.uniform(-0.01, 0.01, m.n_dofs)) == 0
+    c = op.table(0).reshape(-1, 27)
+    jxw = op.table(5).reshape(-1, 27)
+    g = np.array([5.0, 8.0, 5.0]) / 18.0
+    wq = (g[None, None, :] * g[None, :, None] * g[:, None, None]).reshape(-1)
+    ratio = (0.25 ** 3 * wq[None, :]) / jxw * c ** -3.0
+    assert np.max(np.abs(ratio - 1.0)) < 1e-12
