@@ -538,6 +538,73 @@ def c5_measurements(repeats=3):
     return out
 
 
+def dist_vmult_times(cells=N_CELLS_1D, n_parts_list=(2, 4), seed=1234, reps=20):
+    """The distributed operator at the benchmark size on one GPU: the
+    cells^3 Q2 cube split into n z-slab parts (each part's operator on its
+    own stream, ghost update and compress(add) through the in-process
+    group), tensor4 FP64; host wall-clock per vmult over `reps` after 3
+    warm-ups (several streams: synchronised on both sides), against the
+    whole-mesh vmult timed the same way, and the largest difference on the
+    owned entries."""
+    import torch
+    import lsmf
+    kw = dict(geometry="box", coarse=(cells,) * 3, n_refinements=0, degree=DEGREE)
+    gm = lsmf.Mesh(**kw)
+    gm.set_dirichlet([(4, 7)])
+    nc, nn, nd = gm.info()
+    X, _, ijk = gm.arrays()
+    rng = np.random.default_rng(seed)
+    mu = rng.choice([1.0, 10.0], nc)
+    u = smooth_field(X, seed).reshape(-1)
+    src = rng.uniform(-1, 1, nd)
+    gop = lsmf.NeoHookOperator(gm, "tensor4", 1, "fp64")
+    gop.set_material(mu, NU)
+    gop.cache(torch.tensor(u, device="cuda"))
+    dsrc = torch.tensor(src, device="cuda")
+    want = torch.empty_like(dsrc)
+
+    def wall(f):
+        for _ in range(3):
+            f()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(reps):
+            f()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t) / reps * 1e3
+
+    out = {"workload": "%d^3 Q2 cube, tensor4 FP64, z-slab parts on one GPU" % cells, "n_dofs": nd,
+           "whole_ms": round(wall(lambda: gop.vmult(want, dsrc)), 4), "timing": "host wall-clock, synchronised"}
+    want_h = want.cpu().numpy()
+    del gop
+    cell_of = {tuple(c): i for i, c in enumerate(ijk.tolist())}
+    for n_parts in n_parts_list:
+        parts = []
+        for r in range(n_parts):
+            pm = lsmf.Mesh(n_parts=n_parts, part=r, **kw)
+            pm.set_dirichlet([(4, 7)])
+            lay = lsmf.partition_layout(n_parts, r, **kw)
+            _, _, pijk = pm.arrays()
+            gd = (3 * lay["global_node"][:, None] + np.arange(3)).reshape(-1)
+            owned = np.ones(lay["n_nodes"], dtype=bool)
+            owned[lay["upper_shared"]] = False
+            op = lsmf.NeoHookOperator(pm, "tensor4", 1, "fp64")
+            op.set_stream(torch.cuda.Stream())
+            op.set_material(mu[[cell_of[tuple(c)] for c in pijk.tolist()]], NU)
+            op.cache(torch.tensor(u[gd], device="cuda"))
+            s_ = torch.tensor(src[gd], device="cuda")
+            parts.append(dict(op=op, gd=gd, od=(3 * np.nonzero(owned)[0][:, None] + np.arange(3)).reshape(-1),
+                              src=s_, dst=torch.empty_like(s_)))
+        D = lsmf.Dist.group([p["op"] for p in parts])
+        t = wall(lambda: D.vmult([p["dst"] for p in parts], [p["src"] for p in parts]))
+        err = max(float(np.max(np.abs(p["dst"].cpu().numpy()[p["od"]] - want_h[p["gd"][p["od"]]]))) for p in parts)
+        out["parts_%d" % n_parts] = {"ms": round(t, 4), "overhead": round(t / out["whole_ms"] - 1.0, 4),
+                                     "rel_err_owned": err / float(np.max(np.abs(want_h)))}
+        del D, parts
+        torch.cuda.empty_cache()
+    return out
+
+
 def max_over_ranks(t_ms, dist, device):
     """The slowest rank's time (every rank takes part; a single process
     returns its own)."""
@@ -862,8 +929,12 @@ def run_lsmf(args):
     # the large single-GPU configurations: tensor4 vmults at 48^3 Q4 and
     # 128^3 Q2 (24.4 GB of FP64 records)
     large = {}
+    dist_parts = None
     if not args.no_variants and not args.no_large:
         del op
+        torch.cuda.empty_cache()
+        # the z-slab distributed operator at the benchmark size, on this GPU
+        dist_parts = dist_vmult_times(args.cells)
         torch.cuda.empty_cache()
         for cells, degree in ((48, 4), (128, 2)):
             for prec in ("fp64", "fp32"):
@@ -900,7 +971,7 @@ def run_lsmf(args):
                            "l2": "inputs larger than L2 (2.9 GB cache tables), no flush"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": 2 * args.steps, "clocks": clocks, "variants": variants,
-                "stage_split_fp64": stages, "large_vmults": large,
+                "stage_split_fp64": stages, "large_vmults": large, "dist_vmult_one_gpu": dist_parts,
                 "newton_step": newton, "newton_load_steps": load_steps, "adjoint": adjoint}
         print(json.dumps(line), flush=True)
     if dist:

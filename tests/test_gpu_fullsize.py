@@ -7,6 +7,9 @@ oracle is too slow to compare against:
   * the production kernel equals the basic (independent) kernel   (1e-12)
   * every caching variant gives the tensor4 operator              (1e-10)
   * FP32 equals FP64                                               (2e-5)
+  * the z-slab distributed operator (2 and 4 parts on this GPU, ghost
+    update and compress(add)) equals the whole-mesh operator on every
+    owned entry                                                     (1e-12)
 
 Inputs as in bench.py: per-cell mu in {1, 10}, a smooth displacement bounded
 by 0.01 (det F > 0.5), bottom face clamped.
@@ -91,3 +94,10 @@ def test_fp32_equals_fp64(setup):
     ref = _apply(_op(mesh, mu, u), x)
     got = _apply(_op(mesh, mu, u, precision="fp32"), x.float())
     assert _rel(got.double(), ref) < 2e-5
+
+
+def test_partitioned_operator_at_benchmark_size():
+    out = bench.dist_vmult_times(CELLS, (2, 4), reps=2)
+    assert out["n_dofs"] == 6440067
+    for n in (2, 4):
+        assert out["parts_%d" % n]["rel_err_owned"] <= 1e-12, out
