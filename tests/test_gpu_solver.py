@@ -112,14 +112,16 @@ def test_vcycle_graph_follows_each_setup(precision):
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("p", [1, 3, 4])
-def test_vcycle_other_degrees_match_oracle(precision, p):
+@pytest.mark.parametrize("caching", ["tensor4", "tensor2", "scalar_referential"])
+def test_vcycle_other_degrees_match_oracle(precision, p, caching):
     # h-multigrid with Q_p on every level (the transfer maps of degree p, the
-    # level operators' sweeps of degree p)
+    # level operators' sweeps of degree p; FP32 tensor2 at Q1 and
+    # scalar_referential at Q4 run the cell-pair kernel by default)
     coarse, nref = ((2, 2, 2), 2) if p == 1 else ((1, 1, 1), 2)
-    gm, mu, u, dirichlet, (lo, hi), rng = _problem("tensor4", 1, p=p, coarse=coarse, nref=nref)
-    og = O.GMG(O.GEOM_BOX, coarse, nref, lo, hi, 1.0, p, p + 1, "tensor4", 1, precision == "fp32", mu, 0.3,
+    gm, mu, u, dirichlet, (lo, hi), rng = _problem(caching, 1, p=p, coarse=coarse, nref=nref)
+    og = O.GMG(O.GEOM_BOX, coarse, nref, lo, hi, 1.0, p, p + 1, caching, 1, precision == "fp32", mu, 0.3,
                dirichlet, u)
-    g = lsmf.GMG(gm, "tensor4", 1, precision)
+    g = lsmf.GMG(gm, caching, 1, precision)
     g.set_material(mu, 0.3)
     g.setup(torch.tensor(u, device="cuda"))
     tol = 1e-9 if precision == "fp64" else 2e-3
