@@ -183,15 +183,16 @@ lsmf_status lsmf_operator_create(lsmf_mesh *m, int level, lsmf_caching caching, 
   const Level &L = op->L();
   // scalar caching on affine cells: the reference inverse Jacobian is one
   // 3x3 block per cell after the 11 per-point values (c, Eulerian inverse
-  // Jacobian, JxW), the record padded to 16 bytes; otherwise ncomp values
-  // per point
+  // Jacobian, JxW); otherwise ncomp values per point.  Every record is
+  // padded at its end to a multiple of 16 bytes (bulk copies and aligned
+  // records), never with whole components.
   op->ref_per_cell = caching == LSMF_CACHE_SCALAR && L.affine;
+  const int al = 16 / (int)op->elem();
   if (op->ref_per_cell) {
     op->ncomp = 11;
-    const int al = 16 / (int)op->elem();
     op->rec_elems = (11 * L.nq() + 9 + al - 1) / al * al;
   } else {
-    op->rec_elems = op->ncomp * L.nq();
+    op->rec_elems = (op->ncomp * L.nq() + al - 1) / al * al;
   }
   lsmf_status s;
   if ((s = op->d_table.alloc((size_t)L.n_cells * op->rec_elems * op->elem())) != LSMF_OK ||

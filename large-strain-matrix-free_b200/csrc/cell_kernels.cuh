@@ -20,15 +20,16 @@ enum Variant {
 };
 __host__ __device__ constexpr bool variant_referential(int v) { return v == VAR_SCALAR_REF || v == VAR_TENSOR4_NS; }
 
-// Record layout per cell: [comp][qp]; the first 10 components are the metric
-// (inverse Jacobian row-major, JxW) of the frame the variant integrates in:
-// Eulerian for tensor4 / tensor2 / scalar, reference for scalar_referential
-// and tensor4_ns.  Then: tensor4 tau/J (6) + C (36); tensor2 c1, c2, tau/J
-// (6); scalar c + reference inverse Jacobian (9); scalar_referential c + u at
-// the point (3); tensor4_ns dP/dF (81) + 1 pad (16-byte records).
+// Record layout per cell: [comp][qp], ncomp * Q^3 values, the record padded
+// at its end to a multiple of 16 bytes; the first 10 components are the
+// metric (inverse Jacobian row-major, JxW) of the frame the variant
+// integrates in: Eulerian for tensor4 / tensor2 / scalar, reference for
+// scalar_referential and tensor4_ns.  Then: tensor4 tau/J (6) + C (36);
+// tensor2 c1, c2, tau/J (6); scalar c + reference inverse Jacobian (9);
+// scalar_referential c + u at the point (3); tensor4_ns dP/dF (81).
 constexpr int C_JINV = 0, C_JXW = 9, C_VAR = 10;
 __host__ __device__ constexpr int variant_ncomp(int v) {
-  return v == VAR_TENSOR4 ? 52 : v == VAR_TENSOR2 ? 18 : v == VAR_SCALAR_REF ? 14 : v == VAR_TENSOR4_NS ? 92 : 20;
+  return v == VAR_TENSOR4 ? 52 : v == VAR_TENSOR2 ? 18 : v == VAR_SCALAR_REF ? 14 : v == VAR_TENSOR4_NS ? 91 : 20;
 }
 
 template <int P, int Q>

@@ -85,14 +85,14 @@ __global__ void node_sum_kernel(T *dst, const T *__restrict__ buf, const int *__
 
 }  // namespace
 
-// Components per quadrature point of the cell record.  The FP32 tensor2
-// record is padded from 18 to 20 components so that every record is a
-// multiple of 16 bytes (a requirement of the bulk-copy engine).
+// Components per quadrature point of the cell record (the record's length
+// is rounded up to 16 bytes at its end, for the bulk-copy engine).
 int table_components(int caching, int formulation, lsmf_precision precision) {
   (void)formulation;
+  (void)precision;
   if (caching == LSMF_CACHE_TENSOR4) return variant_ncomp(VAR_TENSOR4);
-  if (caching == LSMF_CACHE_TENSOR2) return variant_ncomp(VAR_TENSOR2) + (precision == LSMF_FP32 ? 2 : 0);
-  if (caching == LSMF_CACHE_SCALAR_REFERENTIAL) return variant_ncomp(VAR_SCALAR_REF) + (precision == LSMF_FP32 ? 2 : 0);
+  if (caching == LSMF_CACHE_TENSOR2) return variant_ncomp(VAR_TENSOR2);
+  if (caching == LSMF_CACHE_SCALAR_REFERENTIAL) return variant_ncomp(VAR_SCALAR_REF);
   if (caching == LSMF_CACHE_TENSOR4_NS) return variant_ncomp(VAR_TENSOR4_NS);
   return variant_ncomp(VAR_SCALAR_F1);
 }

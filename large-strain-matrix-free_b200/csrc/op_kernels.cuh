@@ -253,7 +253,6 @@ __global__ void __launch_bounds__(256) cache_kernel(KArgs<T> a, Tab<P, Q> tab) {
                 r[(C_VAR + ((i * 3 + j) * 3 + k) * 3 + l) * NQ] =
                     T(2.0 * lambda * Fi[j][i] * Fi[l][k] + (mu - 2.0 * lambda * lnJ) * Fi[l][i] * Fi[j][k] +
                       (i == k && j == l ? mu : 0.0));
-        r[(C_VAR + 81) * NQ] = T(0);
         continue;
       }
       const double idet = 1.0 / det_F;
