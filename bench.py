@@ -37,17 +37,19 @@ METRIC = "Tangent vmult GDoF/s & Newton-step time, FP32-GMG vs FP64, same 1e-8 r
 
 def alg_bytes(variant, S, n_nodes, n_qp, n_cells):
     """Algorithmic bytes per vmult (values counted once, index maps excluded):
-    scalar S(9N + 11Q + 10C), tensor2 S(6N + 18Q), tensor4 S(6N + 52Q);
+    scalar S(9N + 11Q + 10C), tensor2 S(6N + 17Q), tensor4 S(6N + 51Q);
     the referential variants: scalar_referential S(6N + 14Q) (c, the point
-    displacement, metric), tensor4_ns S(6N + 91Q) (dP/dF, metric)."""
+    displacement, metric), tensor4_ns S(6N + 90Q) (dP/dF, inverse Jacobian).
+    tensor4, tensor2 and tensor4_ns cache their coefficients times JxW, so
+    their records carry no JxW value."""
     if variant == "tensor4":
-        return S * (6 * n_nodes + 52 * n_qp)
+        return S * (6 * n_nodes + 51 * n_qp)
     if variant == "tensor2":
-        return S * (6 * n_nodes + 18 * n_qp)
+        return S * (6 * n_nodes + 17 * n_qp)
     if variant == "scalar_referential":
         return S * (6 * n_nodes + 14 * n_qp)
     if variant == "tensor4_ns":
-        return S * (6 * n_nodes + 91 * n_qp)
+        return S * (6 * n_nodes + 90 * n_qp)
     return S * (9 * n_nodes + 11 * n_qp + 10 * n_cells)
 
 

@@ -193,8 +193,11 @@ lsmf_status lsmf_operator_set_stream(lsmf_op *op, void *stream);
  * Jacobian (9 per qp; Eulerian, or referential for scalar_referential and
  * tensor4_ns), 5 JxW (same frame), 6 scalar_referential displacement values
  * (3 per qp), 7 tensor4_ns dP/dF (81 per qp, index ((i*3+j)*3+k)*3+l);
- * layout [cell][qp][comp] converted to double.  Returns the number of
- * doubles in *count. */
+ * layout [cell][qp][comp] converted to double.  tensor4, tensor2 and
+ * tensor4_ns cache their coefficients multiplied by JxW (the point result
+ * is linear in them): tables 0-3 and 7 of those hold the coefficient times
+ * JxW, and table 5 is LSMF_ERR_INVALID_ARG.  Returns the number of doubles
+ * in *count. */
 lsmf_status lsmf_operator_get_table(lsmf_op *op, int which, double *host, size_t *count);
 
 /* ---- geometric multigrid preconditioner (mf_elasticity.h:1712-2241) ---- */

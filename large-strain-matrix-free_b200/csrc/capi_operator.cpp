@@ -369,15 +369,20 @@ lsmf_status lsmf_operator_get_table(lsmf_op *op, int which, double *host, size_t
   int c0 = 0, nk = 0;
   const bool t4 = op->caching == LSMF_CACHE_TENSOR4, t2 = op->caching == LSMF_CACHE_TENSOR2;
   const bool sr = op->caching == LSMF_CACHE_SCALAR_REFERENTIAL, ns = op->caching == LSMF_CACHE_TENSOR4_NS;
+  // tensor4 / tensor2 / tensor4_ns keep no JxW component: their
+  // coefficients (times JxW) start at component 9
+  const int cv = (t4 || t2 || ns) ? 9 : 10;
   switch (which) {
-    case 0: if (t4 || ns) { set_error("no scalar table"); return LSMF_ERR_INVALID_ARG; } c0 = 10; nk = 1; break;
-    case 1: if (!t2) { set_error("no second scalar table"); return LSMF_ERR_INVALID_ARG; } c0 = 11; nk = 1; break;
-    case 2: if (!t2 && !t4) { set_error("no tensor2 table"); return LSMF_ERR_INVALID_ARG; } c0 = t4 ? 10 : 12; nk = 6; break;
-    case 3: if (!t4) { set_error("no tensor4 table"); return LSMF_ERR_INVALID_ARG; } c0 = 16; nk = 36; break;
+    case 0: if (t4 || ns) { set_error("no scalar table"); return LSMF_ERR_INVALID_ARG; } c0 = cv; nk = 1; break;
+    case 1: if (!t2) { set_error("no second scalar table"); return LSMF_ERR_INVALID_ARG; } c0 = cv + 1; nk = 1; break;
+    case 2: if (!t2 && !t4) { set_error("no tensor2 table"); return LSMF_ERR_INVALID_ARG; } c0 = t4 ? cv : cv + 2; nk = 6; break;
+    case 3: if (!t4) { set_error("no tensor4 table"); return LSMF_ERR_INVALID_ARG; } c0 = cv + 6; nk = 36; break;
     case 4: c0 = 0; nk = 9; break;
-    case 5: c0 = 9; nk = 1; break;
-    case 6: if (!sr) { set_error("no displacement table"); return LSMF_ERR_INVALID_ARG; } c0 = 11; nk = 3; break;
-    case 7: if (!ns) { set_error("no tensor4_ns table"); return LSMF_ERR_INVALID_ARG; } c0 = 10; nk = 81; break;
+    case 5:
+      if (cv == 9) { set_error("JxW is folded into the coefficient tables of this caching"); return LSMF_ERR_INVALID_ARG; }
+      c0 = 9; nk = 1; break;
+    case 6: if (!sr) { set_error("no displacement table"); return LSMF_ERR_INVALID_ARG; } c0 = cv + 1; nk = 3; break;
+    case 7: if (!ns) { set_error("no tensor4_ns table"); return LSMF_ERR_INVALID_ARG; } c0 = cv; nk = 81; break;
     default: set_error("bad table id"); return LSMF_ERR_INVALID_ARG;
   }
   const size_t n = (size_t)L.n_cells * nq * nk;

@@ -21,15 +21,23 @@ enum Variant {
 __host__ __device__ constexpr bool variant_referential(int v) { return v == VAR_SCALAR_REF || v == VAR_TENSOR4_NS; }
 
 // Record layout per cell: [comp][qp], ncomp * Q^3 values, the record padded
-// at its end to a multiple of 16 bytes; the first 10 components are the
-// metric (inverse Jacobian row-major, JxW) of the frame the variant
-// integrates in: Eulerian for tensor4 / tensor2 / scalar, reference for
-// scalar_referential and tensor4_ns.  Then: tensor4 tau/J (6) + C (36);
-// tensor2 c1, c2, tau/J (6); scalar c + reference inverse Jacobian (9);
-// scalar_referential c + u at the point (3); tensor4_ns dP/dF (81).
+// at its end to a multiple of 16 bytes.  The first 9 components are the
+// inverse Jacobian (row-major) of the frame the variant integrates in:
+// Eulerian for tensor4 / tensor2 / scalar, reference for scalar_referential
+// and tensor4_ns.  The point result of tensor4, tensor2 and tensor4_ns is
+// linear in their cached coefficients, so those are stored multiplied by
+// JxW and follow from component 9: tensor4 JxW tau/J (6) + JxW C (36);
+// tensor2 JxW c1, JxW c2, JxW tau/J (6); tensor4_ns JxW dP/dF (81).  The
+// scalar variants keep JxW as component 9, then: scalar c + reference
+// inverse Jacobian (9); scalar_referential c + u at the point (3).
 constexpr int C_JINV = 0, C_JXW = 9, C_VAR = 10;
+__host__ __device__ constexpr bool variant_folds_jxw(int v) {
+  return v == VAR_TENSOR4 || v == VAR_TENSOR2 || v == VAR_TENSOR4_NS;
+}
+// first coefficient component
+__host__ __device__ constexpr int variant_cvar(int v) { return variant_folds_jxw(v) ? C_JXW : C_VAR; }
 __host__ __device__ constexpr int variant_ncomp(int v) {
-  return v == VAR_TENSOR4 ? 52 : v == VAR_TENSOR2 ? 18 : v == VAR_SCALAR_REF ? 14 : v == VAR_TENSOR4_NS ? 91 : 20;
+  return v == VAR_TENSOR4 ? 51 : v == VAR_TENSOR2 ? 17 : v == VAR_SCALAR_REF ? 14 : v == VAR_TENSOR4_NS ? 90 : 20;
 }
 
 template <int P, int Q>
@@ -572,10 +580,12 @@ struct ScalarState {
 
 // Q(g) of do_operation_on_cell (mf_nh_operator.h:922-1499) for the point
 // whose record is rec[comp * NQ] (rec already offset by q; a pointer, or an
-// accessor with operator[] such as the record pair of two cells).
+// accessor with operator[] such as the record pair of two cells); for the
+// variants that fold JxW into their coefficients Q(g) comes out times JxW.
 template <typename T, int VAR, int NQ, typename R>
 __device__ __forceinline__ void physics(const T g[3][3], const R &rec, T mu, T lambda, T kappa,
                                         const ScalarState<T> &st, T Qm[3][3]) {
+  constexpr int CV = variant_cvar(VAR);
   T s[6];
 #pragma unroll
   for (int I = 0; I < 6; ++I) s[I] = T(0.5) * (g[sym_i(I)][sym_j(I)] + g[sym_j(I)][sym_i(I)]);
@@ -584,13 +594,13 @@ __device__ __forceinline__ void physics(const T g[3][3], const R &rec, T mu, T l
     // g * (tau/J) + C : sym(g)     (mf_nh_operator.h:1425-1440)
     T Ts[6];
 #pragma unroll
-    for (int I = 0; I < 6; ++I) Ts[I] = rec[(C_VAR + I) * NQ];
+    for (int I = 0; I < 6; ++I) Ts[I] = rec[(CV + I) * NQ];
     T cs[6];
 #pragma unroll
     for (int I = 0; I < 6; ++I) {
       T a = 0;
 #pragma unroll
-      for (int J = 0; J < 6; ++J) a += rec[(C_VAR + 6 + I * 6 + J) * NQ] * s[J];
+      for (int J = 0; J < 6; ++J) a += rec[(CV + 6 + I * 6 + J) * NQ] * s[J];
       cs[I] = a;
     }
     const T T00 = Ts[0], T11 = Ts[1], T22 = Ts[2], T01 = Ts[3], T02 = Ts[4], T12 = Ts[5];
@@ -606,9 +616,9 @@ __device__ __forceinline__ void physics(const T g[3][3], const R &rec, T mu, T l
     Qm[1][2] += cs[5]; Qm[2][1] += cs[5];
   } else if (VAR == VAR_TENSOR2) {
     // c1 sym(g) + c2 tr(g) I + g * (tau/J)   (mf_nh_operator.h:1401-1424)
-    const T c1 = rec[C_VAR * NQ], c2 = rec[(C_VAR + 1) * NQ];
-    const T T00 = rec[(C_VAR + 2) * NQ], T11 = rec[(C_VAR + 3) * NQ], T22 = rec[(C_VAR + 4) * NQ];
-    const T T01 = rec[(C_VAR + 5) * NQ], T02 = rec[(C_VAR + 6) * NQ], T12 = rec[(C_VAR + 7) * NQ];
+    const T c1 = rec[CV * NQ], c2 = rec[(CV + 1) * NQ];
+    const T T00 = rec[(CV + 2) * NQ], T11 = rec[(CV + 3) * NQ], T22 = rec[(CV + 4) * NQ];
+    const T T01 = rec[(CV + 5) * NQ], T02 = rec[(CV + 6) * NQ], T12 = rec[(CV + 7) * NQ];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       Qm[i][0] = g[i][0] * T00 + g[i][1] * T01 + g[i][2] * T02;
@@ -632,7 +642,7 @@ __device__ __forceinline__ void physics(const T g[3][3], const R &rec, T mu, T l
 #pragma unroll
         for (int k = 0; k < 3; ++k)
 #pragma unroll
-          for (int l = 0; l < 3; ++l) a += rec[(C_VAR + ((i * 3 + j) * 3 + k) * 3 + l) * NQ] * g[k][l];
+          for (int l = 0; l < 3; ++l) a += rec[(CV + ((i * 3 + j) * 3 + k) * 3 + l) * NQ] * g[k][l];
         Qm[i][j] = a;
       }
   } else if (VAR == VAR_SCALAR_REF) {

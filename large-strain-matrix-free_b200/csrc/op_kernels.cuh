@@ -190,17 +190,15 @@ __global__ void __launch_bounds__(256) cache_kernel(KArgs<T> a, Tab<P, Q> tab) {
       inv3(Jr, Jri);
       const double dc = inv3(Jc, Jci);
       T *r = rec + q;
-      if (variant_referential(VAR)) {
-        // scalar_referential / tensor4_ns integrate in the reference frame
-        const double dr = det3(Jr);
+      // scalar_referential / tensor4_ns integrate in the reference frame
+      const double jxw = variant_referential(VAR) ? det3(Jr) * w : dc * w;
 #pragma unroll
-        for (int i = 0; i < 9; ++i) r[(C_JINV + i) * NQ] = T(Jri[i / 3][i % 3]);
-        r[C_JXW * NQ] = T(dr * w);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 9; ++i) r[(C_JINV + i) * NQ] = T(Jci[i / 3][i % 3]);
-        r[C_JXW * NQ] = T(dc * w);
-      }
+      for (int i = 0; i < 9; ++i)
+        r[(C_JINV + i) * NQ] = T(variant_referential(VAR) ? Jri[i / 3][i % 3] : Jci[i / 3][i % 3]);
+      // tensor4 / tensor2 / tensor4_ns store their coefficients times JxW
+      constexpr int CV = variant_cvar(VAR);
+      const double fw = variant_folds_jxw(VAR) ? jxw : 1.0;
+      if (!variant_folds_jxw(VAR)) r[C_JXW * NQ] = T(jxw);
       // F = I + Grad u (reference configuration, mf_nh_operator.h:462-476)
       double F[3][3];
 #pragma unroll
@@ -250,9 +248,9 @@ __global__ void __launch_bounds__(256) cache_kernel(KArgs<T> a, Tab<P, Q> tab) {
           for (int j = 0; j < 3; ++j)
             for (int k = 0; k < 3; ++k)
               for (int l = 0; l < 3; ++l)
-                r[(C_VAR + ((i * 3 + j) * 3 + k) * 3 + l) * NQ] =
-                    T(2.0 * lambda * Fi[j][i] * Fi[l][k] + (mu - 2.0 * lambda * lnJ) * Fi[l][i] * Fi[j][k] +
-                      (i == k && j == l ? mu : 0.0));
+                r[(CV + ((i * 3 + j) * 3 + k) * 3 + l) * NQ] =
+                    T(fw * (2.0 * lambda * Fi[j][i] * Fi[l][k] + (mu - 2.0 * lambda * lnJ) * Fi[l][i] * Fi[j][k] +
+                            (i == k && j == l ? mu : 0.0)));
         continue;
       }
       const double idet = 1.0 / det_F;
@@ -264,20 +262,20 @@ __global__ void __launch_bounds__(256) cache_kernel(KArgs<T> a, Tab<P, Q> tab) {
         tau[I] = mu * b - (i == j ? scalar : 0.0);
       }
       if (VAR == VAR_TENSOR2) {
-        r[C_VAR * NQ] = T(scalar * 2.0 * idet);
-        r[(C_VAR + 1) * NQ] = T(2.0 * lambda * idet);
+        r[CV * NQ] = T(fw * scalar * 2.0 * idet);
+        r[(CV + 1) * NQ] = T(fw * 2.0 * lambda * idet);
 #pragma unroll
-        for (int I = 0; I < 6; ++I) r[(C_VAR + 2 + I) * NQ] = T(tau[I] * idet);
+        for (int I = 0; I < 6; ++I) r[(CV + 2 + I) * NQ] = T(fw * tau[I] * idet);
       } else {
 #pragma unroll
-        for (int I = 0; I < 6; ++I) r[(C_VAR + I) * NQ] = T(tau[I] * idet);
+        for (int I = 0; I < 6; ++I) r[(CV + I) * NQ] = T(fw * tau[I] * idet);
         // C = (2c/J) S + (2 lambda/J) I (x) I  (mf_nh_operator.h:542-546)
         const double ca = scalar * 2.0 * idet, cb = lambda * 2.0 * idet;
 #pragma unroll
         for (int I = 0; I < 6; ++I)
 #pragma unroll
           for (int J = 0; J < 6; ++J)
-            r[(C_VAR + 6 + I * 6 + J) * NQ] = T((I == J ? ca : 0.0) + (I < 3 && J < 3 ? cb : 0.0));
+            r[(CV + 6 + I * 6 + J) * NQ] = T(fw * ((I == J ? ca : 0.0) + (I < 3 && J < 3 ? cb : 0.0)));
       }
     }
     __syncwarp();
@@ -341,7 +339,7 @@ __global__ void __launch_bounds__(256) apply_kernel(KArgs<T> a, Tab<P, Q> tab) {
       T Ji[3][3];
 #pragma unroll
       for (int i = 0; i < 9; ++i) Ji[i / 3][i % 3] = r[(C_JINV + i) * NQ];
-      const T jxw = r[C_JXW * NQ];
+      const T jxw = variant_folds_jxw(VAR) ? T(1) : T(r[C_JXW * NQ]);
       T g[3][3];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
@@ -369,7 +367,10 @@ __global__ void __launch_bounds__(256) apply_kernel(KArgs<T> a, Tab<P, Q> tab) {
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
-        for (int e = 0; e < 3; ++e) H[l][c][e] = (Qm[c][0] * Ji[e][0] + Qm[c][1] * Ji[e][1] + Qm[c][2] * Ji[e][2]) * jxw;
+        for (int e = 0; e < 3; ++e) {
+          const T h = Qm[c][0] * Ji[e][0] + Qm[c][1] * Ji[e][1] + Qm[c][2] * Ji[e][2];
+          H[l][c][e] = variant_folds_jxw(VAR) ? h : T(h * jxw);
+        }
     }
     if (sf) {
       S::integrate(sN, sD, H, V, A, B, lane);
@@ -560,7 +561,7 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
       T Ji[3][3];
 #pragma unroll
       for (int i = 0; i < 9; ++i) Ji[i / 3][i % 3] = r[(C_JINV + i) * NQ];
-      const T jxw = r[C_JXW * NQ];
+      const T jxw = variant_folds_jxw(VAR) ? T(1) : T(r[C_JXW * NQ]);
       T Gq[3][3];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
@@ -594,7 +595,8 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int e = 0; e < 3; ++e) {
-          const T h = (Qm[c][0] * Ji[e][0] + Qm[c][1] * Ji[e][1] + Qm[c][2] * Ji[e][2]) * jxw;
+          const T h0 = Qm[c][0] * Ji[e][0] + Qm[c][1] * Ji[e][1] + Qm[c][2] * Ji[e][2];
+          const T h = variant_folds_jxw(VAR) ? h0 : T(h0 * jxw);
           // each lane overwrites only its own points
           if (PT_SMEM) slab[(c * 3 + e) * S::NQP + q] = h;
           else H[l][c][e] = h;
@@ -773,7 +775,7 @@ __global__ void __launch_bounds__(256) apply_pair_kernel(KArgs<float> a, TabT<P,
       T Ji[3][3];
 #pragma unroll
       for (int i = 0; i < 9; ++i) Ji[i / 3][i % 3] = r[(C_JINV + i) * NQ];
-      const T jxw = r[C_JXW * NQ];
+      const T jxw = variant_folds_jxw(VAR) ? T(1) : T(r[C_JXW * NQ]);
       T Gq[3][3];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
@@ -807,7 +809,8 @@ __global__ void __launch_bounds__(256) apply_pair_kernel(KArgs<float> a, TabT<P,
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int e = 0; e < 3; ++e) {
-          const T h = (Qm[c][0] * Ji[e][0] + Qm[c][1] * Ji[e][1] + Qm[c][2] * Ji[e][2]) * jxw;
+          const T h0 = Qm[c][0] * Ji[e][0] + Qm[c][1] * Ji[e][1] + Qm[c][2] * Ji[e][2];
+          const T h = variant_folds_jxw(VAR) ? h0 : T(h0 * jxw);
           if (PT_SMEM) slab[(c * 3 + e) * S::NQP + q] = h;
           else H[l][c][e] = h;
         }
@@ -885,7 +888,7 @@ __global__ void __launch_bounds__(128) diagonal_kernel(KArgs<T> a, Tab<P, Q> tab
       const int q = lane + 32 * l;
       if (q >= NQ) continue;
       const T *r = rec + q;
-      const T jxw = r[C_JXW * NQ];
+      const T jxw = variant_folds_jxw(VAR) ? T(1) : T(r[C_JXW * NQ]);
       T Ji[3][3];
 #pragma unroll
       for (int i = 0; i < 9; ++i) {
@@ -921,7 +924,8 @@ __global__ void __launch_bounds__(128) diagonal_kernel(KArgs<T> a, Tab<P, Q> tab
           T Qm[3][3];
           physics<T, VAR, NQ>(g, r, mu, lambda, kappa, st, Qm);
 #pragma unroll
-          for (int d = 0; d < 3; ++d) Bq[q * 27 + (c * 3 + d) * 3 + ll] = Qm[c][d] * jxw;
+          for (int d = 0; d < 3; ++d)
+            Bq[q * 27 + (c * 3 + d) * 3 + ll] = variant_folds_jxw(VAR) ? Qm[c][d] : T(Qm[c][d] * jxw);
         }
     }
     __syncwarp();

@@ -112,10 +112,20 @@ def test_cache_tables_match_oracle(caching, formulation):
     op.set_material(mu, 0.3)
     du = torch.tensor(u, device="cuda")
     op.cache(du)
-    whichs = {"tensor4": [2, 3, 4, 5], "tensor2": [0, 1, 2, 4, 5], "scalar": [0, 4, 5],
-              "scalar_referential": [0, 4, 5, 6], "tensor4_ns": [4, 5, 7]}[caching]
+    whichs = {"tensor4": [2, 3, 4], "tensor2": [0, 1, 2, 4], "scalar": [0, 4, 5],
+              "scalar_referential": [0, 4, 5, 6], "tensor4_ns": [4, 7]}[caching]
+    # tensor4 / tensor2 / tensor4_ns store their coefficients times JxW and
+    # no JxW table
+    folded = caching in ("tensor4", "tensor2", "tensor4_ns")
+    jxw = ref.table(5)
     for w in whichs:
-        assert _rel(op.table(w), ref.table(w)) < 1e-13, w
+        want = ref.table(w)
+        if folded and w != 4:
+            want = (want.reshape(jxw.size, -1) * jxw[:, None]).reshape(-1)
+        assert _rel(op.table(w), want) < 1e-13, w
+    if folded:
+        with pytest.raises(lsmf.LsmfError):
+            op.table(5)
 
 
 @pytest.mark.parametrize("caching,formulation", VARIANTS)

@@ -164,9 +164,11 @@ def test_el_n_and_memory_consumption():
     gm, om, cmask, mu, u, src = _setup(p=2, coarse=(2, 2, 2), level=1)
     nc, nn, nd = gm.info()
     # values per cell record: ncomp per quadrature point, padded at the end
-    # to 16 bytes; scalar caching on these affine cells keeps 11 per point
-    # and the reference inverse Jacobian once per cell (11 * 27 + 9 = 306)
-    for caching, rec in (("tensor4", 52 * 27), ("tensor2", 18 * 27), ("scalar", 306), ("tensor4_ns", 91 * 27 + 1)):
+    # to 16 bytes (tensor4, tensor2 and tensor4_ns fold JxW into their
+    # coefficients: 51, 17 and 90 per point); scalar caching on these affine
+    # cells keeps 11 per point and the reference inverse Jacobian once per
+    # cell (11 * 27 + 9 = 306)
+    for caching, rec in (("tensor4", 51 * 27 + 1), ("tensor2", 17 * 27 + 1), ("scalar", 306), ("tensor4_ns", 90 * 27)):
         op = lsmf.NeoHookOperator(gm, caching, 1, "fp64")
         assert op.m() == op.n() == nd
         # cache tables plus the index map and the node coordinates; diagonals
