@@ -543,11 +543,12 @@ def c5_measurements(repeats=3):
 def dist_vmult_times(cells=N_CELLS_1D, n_parts_list=(2, 4), seed=1234, reps=20):
     """The distributed operator at the benchmark size on one GPU: the
     cells^3 Q2 cube split into n z-slab parts (each part's operator on its
-    own stream, ghost update and compress(add) through the in-process
-    group), tensor4 FP64; host wall-clock per vmult over `reps` after 3
-    warm-ups (several streams: synchronised on both sides), against the
-    whole-mesh vmult timed the same way, and the largest difference on the
-    owned entries."""
+    own stream, in-process group), tensor4 FP64, with both interface
+    exchanges: packed (ghost update and compress(add) through buffers) and
+    fused (the cell loops read and add to the neighbours' vectors); host
+    wall-clock per vmult over `reps` after 3 warm-ups (several streams:
+    synchronised on both sides), against the whole-mesh vmult timed the same
+    way, and the largest difference on the owned entries."""
     import torch
     import lsmf
     kw = dict(geometry="box", coarse=(cells,) * 3, n_refinements=0, degree=DEGREE)
@@ -598,10 +599,15 @@ def dist_vmult_times(cells=N_CELLS_1D, n_parts_list=(2, 4), seed=1234, reps=20):
             parts.append(dict(op=op, gd=gd, od=(3 * np.nonzero(owned)[0][:, None] + np.arange(3)).reshape(-1),
                               src=s_, dst=torch.empty_like(s_)))
         D = lsmf.Dist.group([p["op"] for p in parts])
-        t = wall(lambda: D.vmult([p["dst"] for p in parts], [p["src"] for p in parts]))
-        err = max(float(np.max(np.abs(p["dst"].cpu().numpy()[p["od"]] - want_h[p["gd"][p["od"]]]))) for p in parts)
-        out["parts_%d" % n_parts] = {"ms": round(t, 4), "overhead": round(t / out["whole_ms"] - 1.0, 4),
-                                     "rel_err_owned": err / float(np.max(np.abs(want_h)))}
+        rec = {}
+        for mode in ("packed", "fused"):
+            D.set_exchange(mode)
+            t = wall(lambda: D.vmult([p["dst"] for p in parts], [p["src"] for p in parts]))
+            err = max(float(np.max(np.abs(p["dst"].cpu().numpy()[p["od"]] - want_h[p["gd"][p["od"]]])))
+                      for p in parts)
+            rec[mode] = {"ms": round(t, 4), "overhead": round(t / out["whole_ms"] - 1.0, 4),
+                         "rel_err_owned": err / float(np.max(np.abs(want_h)))}
+        out["parts_%d" % n_parts] = rec
         del D, parts
         torch.cuda.empty_cache()
     return out

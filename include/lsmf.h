@@ -312,9 +312,25 @@ lsmf_status lsmf_partition_layout(const lsmf_mesh_desc *desc, int n_parts, int p
                                   int *global_node, int *n_lower, int *lower, int *n_upper, int *upper);
 typedef struct lsmf_dist lsmf_dist;
 /* All parts in this process: ops[r] is the FP64 finest-level operator of
- * part r; each part's work is ordered on its operator's stream, interface
- * buffers move with cudaMemcpyAsync between the parts' streams. */
+ * part r (on any GPU; create it after its mesh's Dirichlet set); each part's
+ * work is ordered on its operator's stream.  The interface exchange is
+ * fused into the cell loops where every part can reach its upper
+ * neighbour's memory (same GPU, or peer access, which this call enables):
+ * the cells next to an interface read the owners' src values and add their
+ * contributions to the owners' dst directly (P2P loads and atomics), with
+ * events ordering the neighbours' streams.  Otherwise the packed exchange
+ * (cudaMemcpyAsync between the parts' streams) is used. */
 lsmf_status lsmf_dist_create_group(int n_parts, lsmf_op *const *ops, lsmf_dist **out);
+/* Interface exchange of the distributed vmult: PACKED (pack, copy / NCCL,
+ * unpack around the cell loops, as update_ghost_values and compress(add))
+ * or FUSED (group objects only, the default where it applies; operators
+ * with the basic kernel or a deterministic scatter use PACKED).  Setting
+ * FUSED where it cannot apply is LSMF_ERR_UNSUPPORTED.  get reports the
+ * form the next vmult uses.  No reference counterpart (deal.II always
+ * exchanges through MPI buffers). */
+enum { LSMF_DIST_EXCHANGE_PACKED = 0, LSMF_DIST_EXCHANGE_FUSED = 1 };
+lsmf_status lsmf_dist_set_exchange(lsmf_dist *d, int mode);
+lsmf_status lsmf_dist_get_exchange(const lsmf_dist *d, int *mode);
 /* One part per process over NCCL (libnccl.so.2 loaded at run time): every
  * process passes the same 128-byte id, made by one of them with
  * lsmf_dist_nccl_unique_id and shared by the host framework. */
@@ -322,9 +338,11 @@ lsmf_status lsmf_dist_nccl_unique_id(unsigned char *id128);
 lsmf_status lsmf_dist_create_nccl(lsmf_op *op, const unsigned char *id128, lsmf_dist **out);
 void lsmf_dist_destroy(lsmf_dist *d);
 /* dst = A src over all parts (arrays of this object's local vectors, one
- * per part it holds): ghost entries of src are set from their owners, the
- * cell loops run, the ghosts' partial sums are added on the owners and the
- * ghost entries of dst cleared.  dst is valid on the owned entries. */
+ * per part it holds): the owners' values of the ghost entries of src are
+ * used by the cell loops, the ghosts' partial sums are added on the owners
+ * and the ghost entries of dst are zero.  dst is valid on the owned
+ * entries.  The packed exchange also sets the ghost entries of src from
+ * their owners; the fused one leaves them as they are. */
 lsmf_status lsmf_dist_vmult(lsmf_dist *d, double *const *dst, double *const *src);
 /* sum over the owned entries of a . b, over all parts (host value) */
 lsmf_status lsmf_dist_dot(lsmf_dist *d, const double *const *a, const double *const *b, double *out);

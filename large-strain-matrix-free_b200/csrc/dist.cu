@@ -12,6 +12,16 @@
 //          dependency on it).
 // Interface data move as packed buffers of 3 values per shared node in the
 // order of the PartLayout lists, which both sides enumerate identically.
+//
+// Fused exchange (group transport, the default where every part can reach
+// its upper neighbour's memory): no packed buffers at all.  Each part's cell
+// loop runs on an index map in which its ghost nodes carry PEER_BIT and the
+// upper neighbour's node numbers, so the interface cells read the owners'
+// src values and add their contributions to the owners' dst over peer
+// memory (NVLink P2P loads and atomics between GPUs; plain device memory
+// when the parts share a GPU).  Ordering is by events between the parts'
+// streams: part r's cell loop starts after part r + 1 has zeroed its dst,
+// and part r + 1 continues after part r's cell loop.
 #include <cuda_runtime.h>
 #include <dlfcn.h>
 #include <nccl.h>
@@ -21,6 +31,7 @@
 #include <new>
 #include <vector>
 
+#include "op_dispatch.h"
 #include "solver_internal.h"
 
 namespace lsmf {
@@ -47,6 +58,19 @@ __global__ void invert_all_kernel(double *inv, const double *d, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     inv[i] = 1.0 / d[i];
 }
+
+// makes a part's device current for the scope (parts of a group may live
+// on different GPUs; streams and allocations belong to their device)
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) cudaSetDevice(dev);
+    else if (prev == dev) prev = -1;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
 
 int grid_of(size_t n) {
   const size_t b = (n + 255) / 256;
@@ -108,16 +132,25 @@ struct lsmf_dist_part {
   DevBuf<double> send_lo, send_up, recv_lo, recv_up;
   DevBuf<double> g, h, d, sc, partial, inv_diag;
   cudaEvent_t ev = nullptr;
+  // fused exchange: the index map with the ghost nodes in the upper
+  // neighbour's numbering (PEER_BIT set; parts with an upper neighbour), the
+  // owned constrained dofs, and the events that order the neighbours' streams
+  DevBuf<int> peer_nodes, con_owned;
+  int n_con_owned = 0;
+  cudaEvent_t ev_zero = nullptr, ev_done = nullptr;
   cudaStream_t stream() const { return op->stream; }
   size_t n() const { return (size_t)op->L().n_dofs(); }
   ~lsmf_dist_part() {
-    if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t e : {ev, ev_zero, ev_done})
+      if (e) cudaEventDestroy(e);
   }
 };
 
 struct lsmf_dist {
   int n_parts = 1;
   bool nccl = false;
+  bool fused_capable = false;  // group: peer maps built, every part reaches its upper neighbour
+  bool fused = false;          // vmults use the fused exchange
   ncclComm_t comm = nullptr;
   std::vector<lsmf_dist_part *> parts;  // group: every part in order; nccl: this process's part
   ~lsmf_dist() {
@@ -133,6 +166,7 @@ lsmf_status init_part(lsmf_dist_part &P, lsmf_op *op) {
   if (!op || op->precision != LSMF_FP64) { set_error("distributed operators must be FP64"); return LSMF_ERR_INVALID_ARG; }
   const PartLayout &Lay = op->mesh->layout;
   if (op->level != (int)op->mesh->levels.size() - 1) { set_error("the operator must be on the finest level"); return LSMF_ERR_INVALID_ARG; }
+  DeviceGuard dg(op->device);
   P.op = op;
   P.part = Lay.part;
   P.n_lower = (int)Lay.lower_shared.size();
@@ -145,13 +179,24 @@ lsmf_status init_part(lsmf_dist_part &P, lsmf_op *op) {
   for (auto *b : {&P.g, &P.h, &P.d, &P.inv_diag}) LSMF_TRY(b->alloc(n));
   LSMF_TRY(P.sc.alloc(SC_N));
   LSMF_TRY(P.partial.alloc(reduce_blocks()));
-  LSMF_CUDA(cudaEventCreateWithFlags(&P.ev, cudaEventDisableTiming));
+  for (cudaEvent_t *e : {&P.ev, &P.ev_zero, &P.ev_done}) LSMF_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  return LSMF_OK;
+}
+
+// run f(i, part) for every part this object holds, each with its device current
+template <typename F>
+lsmf_status each_part(lsmf_dist *D, F &&f) {
+  for (size_t i = 0; i < D->parts.size(); ++i) {
+    DeviceGuard dg(D->parts[i]->op->device);
+    LSMF_TRY(f(i, *D->parts[i]));
+  }
   return LSMF_OK;
 }
 
 lsmf_status pack(lsmf_dist_part &P, const double *v, bool upper, bool zero_constrained) {
   const int n = upper ? P.n_upper : P.n_lower;
   if (!n) return LSMF_OK;
+  DeviceGuard dg(P.op->device);
   pack_kernel<<<grid_of(3 * (size_t)n), 256, 0, P.stream()>>>(v, upper ? P.d_upper.ptr : P.d_lower.ptr, n,
                                                                 P.op->L().d_cmask.ptr, zero_constrained ? 1 : 0,
                                                                 upper ? P.send_up.ptr : P.send_lo.ptr);
@@ -162,6 +207,7 @@ lsmf_status pack(lsmf_dist_part &P, const double *v, bool upper, bool zero_const
 lsmf_status unpack(lsmf_dist_part &P, double *v, bool upper, int mode) {
   const int n = upper ? P.n_upper : P.n_lower;
   if (!n) return LSMF_OK;
+  DeviceGuard dg(P.op->device);
   unpack_kernel<<<grid_of(3 * (size_t)n), 256, 0, P.stream()>>>(v, upper ? P.d_upper.ptr : P.d_lower.ptr, n,
                                                                   upper ? P.recv_up.ptr : P.recv_lo.ptr, mode);
   LSMF_CUDA(cudaGetLastError());
@@ -189,30 +235,38 @@ lsmf_status transfer(lsmf_dist *D, bool down) {
   }
   // group: the receiving part's stream waits for the sender's pack, copies,
   // and the sender's stream waits for the copy before it may pack again
-  for (auto *P : D->parts) LSMF_CUDA(cudaEventRecord(P->ev, P->stream()));
+  LSMF_TRY(each_part(D, [&](size_t, lsmf_dist_part &P) -> lsmf_status {
+    LSMF_CUDA(cudaEventRecord(P.ev, P.stream()));
+    return LSMF_OK;
+  }));
   std::vector<cudaEvent_t> done;
-  for (int r = 0; r < D->n_parts; ++r) {
-    const int from = down ? r + 1 : r - 1;
-    if (from < 0 || from >= D->n_parts) continue;
-    lsmf_dist_part &Rv = *D->parts[r], &Sd = *D->parts[from];
+  lsmf_status st = each_part(D, [&](size_t r, lsmf_dist_part &Rv) -> lsmf_status {
+    const int from = down ? (int)r + 1 : (int)r - 1;
+    if (from < 0 || from >= D->n_parts) return LSMF_OK;
+    lsmf_dist_part &Sd = *D->parts[from];
     const int n = down ? Rv.n_upper : Rv.n_lower;
     if ((down ? Sd.n_lower : Sd.n_upper) != n) { set_error("interface lists of neighbouring parts differ"); return LSMF_ERR_INVALID_ARG; }
     LSMF_CUDA(cudaStreamWaitEvent(Rv.stream(), Sd.ev, 0));
     if (n)
       LSMF_CUDA(cudaMemcpyAsync(down ? Rv.recv_up.ptr : Rv.recv_lo.ptr, down ? Sd.send_lo.ptr : Sd.send_up.ptr,
                                 3 * (size_t)n * sizeof(double), cudaMemcpyDefault, Rv.stream()));
-  }
-  for (int r = 0; r < D->n_parts; ++r) {
-    const int from = down ? r + 1 : r - 1;
-    if (from < 0 || from >= D->n_parts) continue;
     cudaEvent_t e;
     LSMF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    LSMF_CUDA(cudaEventRecord(e, D->parts[r]->stream()));
-    LSMF_CUDA(cudaStreamWaitEvent(D->parts[from]->stream(), e, 0));
     done.push_back(e);
-  }
+    LSMF_CUDA(cudaEventRecord(e, Rv.stream()));
+    return LSMF_OK;
+  });
+  size_t k = 0;
+  if (st == LSMF_OK)
+    st = each_part(D, [&](size_t r, lsmf_dist_part &) -> lsmf_status {
+      const int from = down ? (int)r + 1 : (int)r - 1;
+      if (from < 0 || from >= D->n_parts) return LSMF_OK;
+      // (a stream may wait on an event of another device)
+      LSMF_CUDA(cudaStreamWaitEvent(D->parts[from]->stream(), done[k++], 0));
+      return LSMF_OK;
+    });
   for (cudaEvent_t e : done) cudaEventDestroy(e);
-  return LSMF_OK;
+  return st;
 }
 
 // sum the scalar slot over all parts (every part holds the total afterwards)
@@ -223,15 +277,21 @@ lsmf_status allreduce(lsmf_dist *D, int slot) {
     return LSMF_OK;
   }
   double s = 0;
-  for (auto *P : D->parts) {
+  LSMF_TRY(each_part(D, [&](size_t, lsmf_dist_part &P) -> lsmf_status {
     double v = 0;
-    LSMF_CUDA(cudaMemcpyAsync(&v, P->sc.ptr + slot, sizeof(double), cudaMemcpyDeviceToHost, P->stream()));
-    LSMF_CUDA(cudaStreamSynchronize(P->stream()));
+    LSMF_CUDA(cudaMemcpyAsync(&v, P.sc.ptr + slot, sizeof(double), cudaMemcpyDeviceToHost, P.stream()));
+    LSMF_CUDA(cudaStreamSynchronize(P.stream()));
     s += v;
-  }
-  for (auto *P : D->parts) LSMF_CUDA(cudaMemcpyAsync(P->sc.ptr + slot, &s, sizeof(double), cudaMemcpyHostToDevice, P->stream()));
-  for (auto *P : D->parts) LSMF_CUDA(cudaStreamSynchronize(P->stream()));
-  return LSMF_OK;
+    return LSMF_OK;
+  }));
+  LSMF_TRY(each_part(D, [&](size_t, lsmf_dist_part &P) -> lsmf_status {
+    LSMF_CUDA(cudaMemcpyAsync(P.sc.ptr + slot, &s, sizeof(double), cudaMemcpyHostToDevice, P.stream()));
+    return LSMF_OK;
+  }));
+  return each_part(D, [&](size_t, lsmf_dist_part &P) -> lsmf_status {
+    LSMF_CUDA(cudaStreamSynchronize(P.stream()));
+    return LSMF_OK;
+  });
 }
 
 // ghost entries (upper-shared nodes) of v from their owners
@@ -255,10 +315,106 @@ lsmf_status compress_add(lsmf_dist *D, double *const *v) {
   return LSMF_OK;
 }
 
+// Build the fused exchange of a group: every part's upper neighbour must be
+// reachable (same GPU, or peer access enabled between the two GPUs); the
+// index map of a part with an upper neighbour renumbers its ghost nodes
+// into the neighbour's numbering (the interface lists of both sides are in
+// the same order).  Leaves D->fused_capable false when it does not apply.
+lsmf_status setup_fused(lsmf_dist *D) {
+  const int n = (int)D->parts.size();
+  if (D->nccl || n < 2) return LSMF_OK;
+  for (int r = 0; r + 1 < n; ++r) {
+    const int da = D->parts[r]->op->device, db = D->parts[r + 1]->op->device;
+    if (da == db) continue;
+    int can = 0;
+    LSMF_CUDA(cudaDeviceCanAccessPeer(&can, da, db));
+    if (!can) return LSMF_OK;
+    DeviceGuard dg(da);
+    const cudaError_t e = cudaDeviceEnablePeerAccess(db, 0);
+    if (e == cudaErrorPeerAccessAlreadyEnabled) (void)cudaGetLastError();
+    else if (e != cudaSuccess) { (void)cudaGetLastError(); return LSMF_OK; }
+  }
+  for (int r = 0; r < n; ++r) {
+    lsmf_dist_part &P = *D->parts[r];
+    const Level &L = P.op->L();
+    if (L.n_nodes > PEER_NODE_MASK) return LSMF_OK;
+    const PartLayout &Lay = P.op->mesh->layout;
+    std::vector<int> ghost_of(L.n_nodes, -1);
+    for (size_t j = 0; j < Lay.upper_shared.size(); ++j) ghost_of[Lay.upper_shared[j]] = (int)j;
+    DeviceGuard dg(P.op->device);
+    // identity rows of the owned constrained dofs (a ghost's row is its owner's)
+    std::vector<int> con;
+    for (int dof : L.constrained)
+      if (ghost_of[dof / 3] < 0) con.push_back(dof);
+    P.n_con_owned = (int)con.size();
+    LSMF_TRY(P.con_owned.upload(con.data(), con.size()));
+    if (r + 1 == n) continue;
+    const std::vector<int> &owner = D->parts[r + 1]->op->mesh->layout.lower_shared;
+    if (owner.size() != Lay.upper_shared.size()) { set_error("interface lists of neighbouring parts differ"); return LSMF_ERR_INVALID_ARG; }
+    std::vector<int> packed(L.cell_nodes.size());
+    for (size_t i = 0; i < packed.size(); ++i) {
+      const int node = L.cell_nodes[i];
+      const int cm = L.cmask[3 * (size_t)node] | (L.cmask[3 * (size_t)node + 1] << 1) |
+                     (L.cmask[3 * (size_t)node + 2] << 2);
+      const int j = ghost_of[node];
+      packed[i] = (j < 0 ? node : (PEER_BIT | owner[j])) | (cm << NODE_BITS);
+    }
+    LSMF_TRY(P.peer_nodes.upload(packed.data(), packed.size()));
+  }
+  D->fused_capable = true;
+  D->fused = true;
+  return LSMF_OK;
+}
+
+// the fused exchange serves operators with the fast kernel and atomic scatter
+bool fused_applies(const lsmf_dist *D) {
+  if (!D->fused) return false;
+  for (auto *P : D->parts)
+    if (P->op->basic || P->op->scatter != LSMF_SCATTER_ATOMIC) return false;
+  return true;
+}
+
+// dst = A src with the interface exchange done by the cell loops (fused):
+// zero every dst; part r's cell loop, once part r + 1 has zeroed its dst,
+// gathers its ghosts from src[r + 1] and adds their contributions to
+// dst[r + 1]; part r + 1 continues after it.  dst's ghost entries stay zero
+// and src's ghost entries are not read.
+lsmf_status dist_vmult_fused(lsmf_dist *D, double *const *dst, double *const *src) {
+  const int n = (int)D->parts.size();
+  LSMF_TRY(each_part(D, [&](size_t r, lsmf_dist_part &P) -> lsmf_status {
+    LSMF_CUDA(cudaMemsetAsync(dst[r], 0, P.n() * sizeof(double), P.stream()));
+    LSMF_CUDA(cudaEventRecord(P.ev_zero, P.stream()));
+    return LSMF_OK;
+  }));
+  LSMF_TRY(each_part(D, [&](size_t r, lsmf_dist_part &P) -> lsmf_status {
+    if ((int)r + 1 < n) {
+      lsmf_dist_part &U = *D->parts[r + 1];
+      LSMF_CUDA(cudaStreamWaitEvent(P.stream(), U.ev_zero, 0));
+      CellRange rg;
+      rg.peer_nodes = P.peer_nodes.ptr;
+      rg.peer_src = src[r + 1];
+      rg.peer_dst = dst[r + 1];
+      rg.peer_u = U.op->d_u;
+      LSMF_TRY(launch_apply_peer(P.op, dst[r], src[r], rg, P.con_owned.ptr, P.n_con_owned));
+    } else {
+      // the top part has no ghosts: the plain cell loop, dst already zero
+      LSMF_TRY(launch_apply(P.op, dst[r], src[r], LSMF_MASK_DEFAULT, true));
+    }
+    LSMF_CUDA(cudaEventRecord(P.ev_done, P.stream()));
+    return LSMF_OK;
+  }));
+  return each_part(D, [&](size_t r, lsmf_dist_part &P) -> lsmf_status {
+    if (r > 0) LSMF_CUDA(cudaStreamWaitEvent(P.stream(), D->parts[r - 1]->ev_done, 0));
+    return LSMF_OK;
+  });
+}
+
 lsmf_status dist_vmult(lsmf_dist *D, double *const *dst, double *const *src) {
+  if (fused_applies(D)) return dist_vmult_fused(D, dst, src);
   LSMF_TRY(update_ghosts(D, src));
-  for (size_t i = 0; i < D->parts.size(); ++i)
-    LSMF_TRY(launch_apply(D->parts[i]->op, dst[i], src[i], LSMF_MASK_DEFAULT, false));
+  LSMF_TRY(each_part(D, [&](size_t i, lsmf_dist_part &P) -> lsmf_status {
+    return launch_apply(P.op, dst[i], src[i], LSMF_MASK_DEFAULT, false);
+  }));
   return compress_add(D, dst);
 }
 
@@ -283,7 +439,29 @@ lsmf_status lsmf_dist_create_group(int n_parts, lsmf_op *const *ops, lsmf_dist *
     lsmf_status s = init_part(*D->parts.back(), ops[r]);
     if (s != LSMF_OK) { delete D; return s; }
   }
+  lsmf_status s = setup_fused(D);
+  if (s != LSMF_OK) { delete D; return s; }
   *out = D;
+  return LSMF_OK;
+}
+
+lsmf_status lsmf_dist_set_exchange(lsmf_dist *D, int mode) {
+  if (!D || (mode != LSMF_DIST_EXCHANGE_PACKED && mode != LSMF_DIST_EXCHANGE_FUSED)) {
+    set_error("bad arguments");
+    return LSMF_ERR_INVALID_ARG;
+  }
+  if (mode == LSMF_DIST_EXCHANGE_FUSED && !D->fused_capable) {
+    set_error("the fused exchange needs every part in this process with its upper neighbour reachable (same GPU "
+              "or peer access) and fewer than 2^28 nodes per part");
+    return LSMF_ERR_UNSUPPORTED;
+  }
+  D->fused = mode == LSMF_DIST_EXCHANGE_FUSED;
+  return LSMF_OK;
+}
+
+lsmf_status lsmf_dist_get_exchange(const lsmf_dist *D, int *mode) {
+  if (!D || !mode) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  *mode = fused_applies(D) ? LSMF_DIST_EXCHANGE_FUSED : LSMF_DIST_EXCHANGE_PACKED;
   return LSMF_OK;
 }
 
@@ -311,6 +489,7 @@ lsmf_status lsmf_dist_create_nccl(lsmf_op *op, const unsigned char *id128, lsmf_
   if (s != LSMF_OK) { delete D; return s; }
   ncclUniqueId id;
   std::memcpy(&id, id128, sizeof(id));
+  DeviceGuard dg(op->device);
   const ncclResult_t r = g_nccl.CommInitRank(&D->comm, Lay.n_parts, id, Lay.part);
   if (r != ncclSuccess) {
     set_error(std::string("ncclCommInitRank: ") + g_nccl.GetErrorString(r));
@@ -335,15 +514,15 @@ lsmf_status lsmf_dist_dot(lsmf_dist *D, const double *const *a, const double *co
   if (!D || !a || !b || !out) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
   // owned entries only: b is copied into a work vector whose ghost entries
   // are cleared, so each part sums over the entries it owns
-  for (size_t i = 0; i < D->parts.size(); ++i) {
-    lsmf_dist_part &P = *D->parts[i];
+  LSMF_TRY(each_part(D, [&](size_t i, lsmf_dist_part &P) -> lsmf_status {
     LSMF_CUDA(cudaMemcpyAsync(P.g.ptr, b[i], P.n() * sizeof(double), cudaMemcpyDeviceToDevice, P.stream()));
     LSMF_TRY(pack(P, P.g.ptr, true, false));
     LSMF_TRY(unpack(P, P.g.ptr, true, 2));
-    LSMF_TRY(dot_async(a[i], P.g.ptr, false, P.n(), P.partial.ptr, P.sc.ptr, SC_TMP, P.stream()));
-  }
+    return dot_async(a[i], P.g.ptr, false, P.n(), P.partial.ptr, P.sc.ptr, SC_TMP, P.stream());
+  }));
   LSMF_TRY(allreduce(D, SC_TMP));
   lsmf_dist_part &P0 = *D->parts[0];
+  DeviceGuard dg(P0.op->device);
   LSMF_CUDA(cudaMemcpyAsync(out, P0.sc.ptr + SC_TMP, sizeof(double), cudaMemcpyDeviceToHost, P0.stream()));
   LSMF_CUDA(cudaStreamSynchronize(P0.stream()));
   return LSMF_OK;
@@ -366,21 +545,20 @@ lsmf_status lsmf_dist_cg_solve(lsmf_dist *D, int precond, double omega, double *
   if (precond == 1) {
     // the diagonal of the whole operator on the owned entries: each part's
     // cell contributions, compress(add) across the interfaces, then inverted
-    for (size_t i = 0; i < np; ++i) {
-      lsmf_dist_part &P = *D->parts[i];
+    LSMF_TRY(each_part(D, [&](size_t i, lsmf_dist_part &P) -> lsmf_status {
       LSMF_TRY(lsmf_operator_compute_diagonal(P.op));
       LSMF_CUDA(cudaMemcpyAsync(h[i], P.op->d_diag.ptr, P.n() * sizeof(double), cudaMemcpyDeviceToDevice, P.stream()));
-    }
+      return LSMF_OK;
+    }));
     LSMF_TRY(compress_add(D, h.data()));
     LSMF_TRY(update_ghosts(D, h.data()));
-    for (size_t i = 0; i < np; ++i) {
-      lsmf_dist_part &P = *D->parts[i];
+    LSMF_TRY(each_part(D, [&](size_t i, lsmf_dist_part &P) -> lsmf_status {
       invert_all_kernel<<<grid_of(P.n()), 256, 0, P.stream()>>>(invd[i], h[i], P.n());
       LSMF_CUDA(cudaGetLastError());
-    }
+      return LSMF_OK;
+    }));
   }
-  auto prec = [&](size_t i) -> lsmf_status {
-    lsmf_dist_part &P = *D->parts[i];
+  auto prec = [&](size_t i, lsmf_dist_part &P) -> lsmf_status {
     if (precond == 0) {
       LSMF_CUDA(cudaMemcpyAsync(h[i], g[i], P.n() * sizeof(double), cudaMemcpyDeviceToDevice, P.stream()));
       return LSMF_OK;
@@ -389,19 +567,19 @@ lsmf_status lsmf_dist_cg_solve(lsmf_dist *D, int precond, double omega, double *
   };
   auto read = [&](int slot, double &v) -> lsmf_status {
     lsmf_dist_part &P = *D->parts[0];
+    DeviceGuard dg(P.op->device);
     LSMF_CUDA(cudaMemcpyAsync(&v, P.sc.ptr + slot, sizeof(double), cudaMemcpyDeviceToHost, P.stream()));
     LSMF_CUDA(cudaStreamSynchronize(P.stream()));
     return LSMF_OK;
   };
   // g = A x - b with zero ghost entries
   LSMF_TRY(dist_vmult(D, h.data(), x));
-  for (size_t i = 0; i < np; ++i) {
-    lsmf_dist_part &P = *D->parts[i];
+  LSMF_TRY(each_part(D, [&](size_t i, lsmf_dist_part &P) -> lsmf_status {
     LSMF_TRY(neg_residual_async<double>(g[i], h[i], b[i], P.n(), P.stream()));
     LSMF_TRY(pack(P, g[i], true, false));
     LSMF_TRY(unpack(P, g[i], true, 2));
-    LSMF_TRY(dot_async(g[i], g[i], false, P.n(), P.partial.ptr, P.sc.ptr, SC_RES2, P.stream()));
-  }
+    return dot_async(g[i], g[i], false, P.n(), P.partial.ptr, P.sc.ptr, SC_RES2, P.stream());
+  }));
   LSMF_TRY(allreduce(D, SC_RES2));
   double res2 = 0;
   LSMF_TRY(read(SC_RES2, res2));
@@ -409,47 +587,48 @@ lsmf_status lsmf_dist_cg_solve(lsmf_dist *D, int precond, double omega, double *
   int it = 0;
   bool conv = res <= tol_abs;
   if (!conv && max_it > 0) {
-    for (size_t i = 0; i < np; ++i) {
-      LSMF_TRY(prec(i));
-      LSMF_TRY(dot_async(g[i], h[i], false, D->parts[i]->n(), D->parts[i]->partial.ptr, D->parts[i]->sc.ptr, SC_GH0,
-                         D->parts[i]->stream()));
-    }
+    LSMF_TRY(each_part(D, [&](size_t i, lsmf_dist_part &P) -> lsmf_status {
+      LSMF_TRY(prec(i, P));
+      return dot_async(g[i], h[i], false, P.n(), P.partial.ptr, P.sc.ptr, SC_GH0, P.stream());
+    }));
     LSMF_TRY(allreduce(D, SC_GH0));
-    for (size_t i = 0; i < np; ++i)
-      LSMF_TRY(cg_dir_async(d[i], h[i], D->parts[i]->n(), D->parts[i]->sc.ptr, SC_GH0, SC_GH0, true,
-                            D->parts[i]->stream()));
+    LSMF_TRY(each_part(D, [&](size_t i, lsmf_dist_part &P) -> lsmf_status {
+      return cg_dir_async(d[i], h[i], P.n(), P.sc.ptr, SC_GH0, SC_GH0, true, P.stream());
+    }));
     int k = 0;
     while (true) {
       ++it;
       LSMF_TRY(dist_vmult(D, h.data(), d.data()));
-      for (size_t i = 0; i < np; ++i)
-        LSMF_TRY(dot_async(d[i], h[i], false, D->parts[i]->n(), D->parts[i]->partial.ptr, D->parts[i]->sc.ptr, SC_DH,
-                           D->parts[i]->stream()));
+      LSMF_TRY(each_part(D, [&](size_t i, lsmf_dist_part &P) -> lsmf_status {
+        return dot_async(d[i], h[i], false, P.n(), P.partial.ptr, P.sc.ptr, SC_DH, P.stream());
+      }));
       LSMF_TRY(allreduce(D, SC_DH));
-      for (size_t i = 0; i < np; ++i)
-        LSMF_TRY(cg_update_async(x[i], g[i], d[i], h[i], D->parts[i]->n(), D->parts[i]->sc.ptr, SC_GH0 + (k & 1),
-                                 D->parts[i]->partial.ptr, D->parts[i]->stream()));
+      LSMF_TRY(each_part(D, [&](size_t i, lsmf_dist_part &P) -> lsmf_status {
+        return cg_update_async(x[i], g[i], d[i], h[i], P.n(), P.sc.ptr, SC_GH0 + (k & 1), P.partial.ptr, P.stream());
+      }));
       LSMF_TRY(allreduce(D, SC_RES2));
       LSMF_TRY(read(SC_RES2, res2));
       res = std::sqrt(res2);
       if (!(res == res)) break;
       if (res <= tol_abs) { conv = true; break; }
       if (it >= max_it) break;
-      for (size_t i = 0; i < np; ++i) {
-        LSMF_TRY(prec(i));
-        LSMF_TRY(dot_async(g[i], h[i], false, D->parts[i]->n(), D->parts[i]->partial.ptr, D->parts[i]->sc.ptr,
-                           SC_GH0 + ((k + 1) & 1), D->parts[i]->stream()));
-      }
+      LSMF_TRY(each_part(D, [&](size_t i, lsmf_dist_part &P) -> lsmf_status {
+        LSMF_TRY(prec(i, P));
+        return dot_async(g[i], h[i], false, P.n(), P.partial.ptr, P.sc.ptr, SC_GH0 + ((k + 1) & 1), P.stream());
+      }));
       LSMF_TRY(allreduce(D, SC_GH0 + ((k + 1) & 1)));
-      for (size_t i = 0; i < np; ++i)
-        LSMF_TRY(cg_dir_async(d[i], h[i], D->parts[i]->n(), D->parts[i]->sc.ptr, SC_GH0 + ((k + 1) & 1),
-                              SC_GH0 + (k & 1), false, D->parts[i]->stream()));
+      LSMF_TRY(each_part(D, [&](size_t i, lsmf_dist_part &P) -> lsmf_status {
+        return cg_dir_async(d[i], h[i], P.n(), P.sc.ptr, SC_GH0 + ((k + 1) & 1), SC_GH0 + (k & 1), false, P.stream());
+      }));
       ++k;
     }
   }
   // the owners' values in the ghost entries of the solution
   LSMF_TRY(update_ghosts(D, x));
-  for (auto *P : D->parts) LSMF_CUDA(cudaStreamSynchronize(P->stream()));
+  LSMF_TRY(each_part(D, [&](size_t, lsmf_dist_part &P) -> lsmf_status {
+    LSMF_CUDA(cudaStreamSynchronize(P.stream()));
+    return LSMF_OK;
+  }));
   if (info) { info->iterations = it; info->residual = res; info->converged = conv ? 1 : 0; }
   if (!conv) { set_error("CG did not reach the tolerance"); return LSMF_ERR_CG_NOT_CONVERGED; }
   return LSMF_OK;

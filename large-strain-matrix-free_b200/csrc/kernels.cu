@@ -208,6 +208,29 @@ lsmf_status launch_apply(const lsmf_op *op, void *dst, const void *src, unsigned
   return LSMF_OK;
 }
 
+// Cell loop of a partitioned FP64 vmult with the interface exchange fused
+// in (range.peer_*: the ghost nodes' values are read from, and their
+// contributions added to, the neighbour part's vectors), then the identity
+// rows of the part's owned constrained dofs d_con[0 .. n_con).  dst is not
+// zeroed here: the caller orders the zeroing of this part's and of the
+// neighbour's dst before the launch.
+lsmf_status launch_apply_peer(const lsmf_op *op, double *dst, const double *src, const CellRange &range,
+                              const int *d_con, int n_con) {
+  const OpsTable *t = table_of(op);
+  if (!t) return LSMF_ERR_UNSUPPORTED;
+  if (op->precision != LSMF_FP64 || op->basic || op->scatter != LSMF_SCATTER_ATOMIC || !range.peer_nodes) {
+    set_error("the fused interface exchange needs an FP64 operator with the fast kernel and atomic scatter");
+    return LSMF_ERR_INVALID_ARG;
+  }
+  LSMF_TRY(t->apply(op, dst, src, LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD, range));
+  if (n_con) {
+    const int g = (n_con + 255) / 256 < 4 * num_sms() ? (n_con + 255) / 256 : 4 * num_sms();
+    constrained_add_kernel<double><<<g, 256, 0, op->stream>>>(dst, src, d_con, n_con);
+    LSMF_CUDA(cudaGetLastError());
+  }
+  return LSMF_OK;
+}
+
 lsmf_status launch_apply_cells(const lsmf_op *op, void *dst, const void *src) {
   const OpsTable *t = table_of(op);
   if (!t) return LSMF_ERR_UNSUPPORTED;

@@ -36,6 +36,11 @@ void set_error(const std::string &msg);
 
 constexpr int NODE_BITS = 29;
 constexpr int NODE_MASK = (1 << NODE_BITS) - 1;
+// index maps of a partitioned operator's fused interface exchange: a node
+// with PEER_BIT set is the neighbour part's node PEER_BIT ^ id (its vectors
+// are read and added to directly); nodes stay below PEER_BIT
+constexpr int PEER_BIT = 1 << (NODE_BITS - 1);
+constexpr int PEER_NODE_MASK = PEER_BIT - 1;
 
 // 1D Lagrange basis on Gauss-Lobatto nodes at Gauss points on [0,1].
 struct Basis {

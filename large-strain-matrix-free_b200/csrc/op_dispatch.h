@@ -17,6 +17,14 @@ struct CellRange {
   int n_list = 0;
   bool plain = false;
   void *cellbuf = nullptr;
+  // fused interface exchange of a partitioned FP64 vmult (full cell loop,
+  // atomic scatter): `peer_nodes` replaces the level's index map; its nodes
+  // with PEER_BIT are the neighbour part's, gathered from peer_src / peer_u
+  // and added to peer_dst (device pointers the launching device can reach)
+  const int *peer_nodes = nullptr;
+  const void *peer_src = nullptr;
+  void *peer_dst = nullptr;
+  const void *peer_u = nullptr;
 };
 
 struct OpsTable {
@@ -41,6 +49,11 @@ template <> const OpsTable &ops_table<3, double>();
 template <> const OpsTable &ops_table<3, float>();
 template <> const OpsTable &ops_table<4, double>();
 template <> const OpsTable &ops_table<4, float>();
+
+// the partitioned vmult's cell loop with the fused interface exchange
+// (kernels.cu)
+lsmf_status launch_apply_peer(const lsmf_op *op, double *dst, const double *src, const CellRange &range,
+                              const int *d_con, int n_con);
 
 // the table of a level's degree and an operator's precision (nullptr for an
 // unsupported degree)

@@ -45,6 +45,11 @@ struct KArgs {
   const int *cells;      // cell list of one colour (nullptr: all n_cells cells)
   int plain;             // scatter with plain adds (colour launches) instead of atomics
   T *cellbuf;            // node-sum scatter: per-cell results [cell][local node][component]
+  // fused interface exchange (SC_PEER): the neighbour part's vectors, read
+  // and added to for the nodes with PEER_BIT in cell_nodes
+  const T *psrc;
+  T *pdst;
+  const T *pu;
 };
 
 // cell of list entry i
@@ -407,8 +412,11 @@ __global__ void __launch_bounds__(256) apply_kernel(KArgs<T> a, Tab<P, Q> tab) {
 // cell list of one lattice colour (a.cells, a.n_cells entries) with plain
 // adds; SC_CELLBUF over all cells, storing every cell's results to
 // a.cellbuf[cell][local node][component] (constrained rows as zero) for the
-// node sum that follows.
-constexpr int SC_ATOMIC = 0, SC_COLOUR = 1, SC_CELLBUF = 2;
+// node sum that follows; SC_PEER as SC_ATOMIC, with the neighbour part's
+// nodes (PEER_BIT in the index map) gathered from a.psrc / a.pu and added to
+// a.pdst over peer memory: the partitioned vmult's ghost update and
+// compress(add) done by the cell loop itself.
+constexpr int SC_ATOMIC = 0, SC_COLOUR = 1, SC_CELLBUF = 2, SC_PEER = 3;
 template <int P, int Q, typename T, int VAR, int STAGES, int SC>
 __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, T> tab) {
   constexpr bool COL = SC == SC_COLOUR;
@@ -478,9 +486,16 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
         for (int i = 0; i < N1; ++i) {
           const int packed = __ldg(cn + kj * N1 + i);
           pk[r][i] = packed;
-          const size_t dof = 3 * (size_t)(packed & NODE_MASK) + comp;
-          pv[r][i] = __ldg(a.src + dof);
-          if (SCALAR) pu[r][i] = __ldg(a.u + dof);
+          if (SC == SC_PEER) {
+            const bool pe = packed & PEER_BIT;
+            const size_t dof = 3 * (size_t)(packed & PEER_NODE_MASK) + comp;
+            pv[r][i] = __ldg((pe ? a.psrc : a.src) + dof);
+            if (SCALAR) pu[r][i] = __ldg((pe ? a.pu : a.u) + dof);
+          } else {
+            const size_t dof = 3 * (size_t)(packed & NODE_MASK) + comp;
+            pv[r][i] = __ldg(a.src + dof);
+            if (SCALAR) pu[r][i] = __ldg(a.u + dof);
+          }
         }
       }
     }
@@ -628,6 +643,11 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
           const bool con = (ck[r][i] >> (NODE_BITS + comp)) & 1;
           if (SC == SC_CELLBUF) {
             a.cellbuf[((size_t)cell * NN + (xk * N1 + xj) * N1 + i) * 3 + comp] = con ? T(0) : out[r][i];
+          } else if (SC == SC_PEER) {
+            if (!con) {
+              const int k = ck[r][i];
+              atomic_add(((k & PEER_BIT) ? a.pdst : a.dst) + 3 * (size_t)(k & PEER_NODE_MASK) + comp, out[r][i]);
+            }
           } else if (!con) {
             T *d = a.dst + 3 * (size_t)(ck[r][i] & NODE_MASK) + comp;
             if (COL) *d += out[r][i];
@@ -1054,6 +1074,9 @@ KArgs<T> make_args(const lsmf_op *op) {
   a.plain = 0;
   a.cellbuf = nullptr;
   a.prefetch = op->prefetch;
+  a.psrc = nullptr;
+  a.pdst = nullptr;
+  a.pu = nullptr;
   return a;
 }
 
@@ -1065,6 +1088,12 @@ void set_range(KArgs<T> &a, const CellRange &r) {
   }
   a.plain = r.plain ? 1 : 0;
   a.cellbuf = (T *)r.cellbuf;
+  if (r.peer_nodes) {
+    a.cell_nodes = r.peer_nodes;
+    a.psrc = (const T *)r.peer_src;
+    a.pdst = (T *)r.peer_dst;
+    a.pu = (const T *)r.peer_u;
+  }
 }
 
 template <int P, int Q, typename T, int VAR>
@@ -1143,8 +1172,13 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
     set_error("the node-sum scatter serves the full vmult cell loop only");
     return LSMF_ERR_INVALID_ARG;
   }
-  // the colour and cell-buffer launches are built with at most one stage
-  if ((col || cellbuf) && stages > 1) stages = 1;
+  const bool peer = range.peer_nodes != nullptr;
+  if (peer && (!full || op->basic || col || cellbuf || sizeof(T) != 8)) {
+    set_error("the fused interface exchange serves the full FP64 vmult cell loop with atomic scatter only");
+    return LSMF_ERR_INVALID_ARG;
+  }
+  // the colour, cell-buffer and peer launches are built with at most one stage
+  if ((col || cellbuf || peer) && stages > 1) stages = 1;
   if constexpr (std::is_same<T, float>::value) {
     // automatic choice, measured on B200 (FP32 vmult at 96^3 Q1, 64^3 Q2,
     // 48^3 Q3 / Q4 and the 15^3 -> 30^3 / 60^3 Q2 V-cycles), pairs where
@@ -1194,6 +1228,10 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
     } else if (cellbuf) {
       st = stages == 0 ? go(apply_fast_kernel<P, Q, T, VAR, 0, SC_CELLBUF>)
                        : go(apply_fast_kernel<P, Q, T, VAR, 1, SC_CELLBUF>);
+    } else if (peer) {
+      if constexpr (sizeof(T) == 8)
+        st = stages == 0 ? go(apply_fast_kernel<P, Q, T, VAR, 0, SC_PEER>)
+                         : go(apply_fast_kernel<P, Q, T, VAR, 1, SC_PEER>);
     } else {
       switch (stages) {
         case 0: st = go(apply_fast_kernel<P, Q, T, VAR, 0, SC_ATOMIC>); break;

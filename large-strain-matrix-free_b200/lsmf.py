@@ -119,6 +119,8 @@ SIGNATURES = {
     "lsmf_dist_create_nccl": (ctypes.c_int, [vp, vp, ctypes.POINTER(vp)]),
     "lsmf_dist_destroy": (None, [vp]),
     "lsmf_dist_vmult": (ctypes.c_int, [vp, vp, vp]),
+    "lsmf_dist_set_exchange": (ctypes.c_int, [vp, ctypes.c_int]),
+    "lsmf_dist_get_exchange": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int)]),
     "lsmf_dist_dot": (ctypes.c_int, [vp, vp, vp, dp]),
     "lsmf_dist_cg_solve": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, vp, vp, ctypes.c_double, ctypes.c_int,
                                           ctypes.POINTER(SolveInfo)]),
@@ -493,6 +495,19 @@ class Dist:
 
     def __del__(self, _release=_release):  # bound now: module globals are gone at exit
         _release(self, "lsmf_dist_destroy")
+
+    EXCHANGE = {"packed": 0, "fused": 1}
+
+    def set_exchange(self, mode):
+        """"packed" (update_ghost_values / compress(add) through buffers) or
+        "fused" (group objects: the cell loops read and add to the
+        neighbours' vectors directly)."""
+        check(lib().lsmf_dist_set_exchange(self.h, self.EXCHANGE[mode] if isinstance(mode, str) else int(mode)))
+
+    def exchange(self):
+        m = ctypes.c_int()
+        check(lib().lsmf_dist_get_exchange(self.h, ctypes.byref(m)))
+        return {v: k for k, v in self.EXCHANGE.items()}[m.value]
 
     def vmult(self, dsts, srcs):
         check(lib().lsmf_dist_vmult(self.h, _ptr_array(dsts), _ptr_array(srcs)))

@@ -1,9 +1,12 @@
 """The distributed operator on one GPU: z-slab parts driven by one process
-(lsmf_dist_create_group), each part's operator on its own CUDA stream, the
-interface buffers moved between the parts' streams on the device.
+(lsmf_dist_create_group), each part's operator on its own CUDA stream, with
+both interface exchanges: packed (update_ghost_values / compress(add)
+through buffers moved between the parts' streams) and fused (the cell loops
+read the owners' src values and add to the owners' dst directly, the
+neighbours' streams ordered by events).
 
-* vmult (update_ghost_values, cell loops, compress(add)) equals the
-  whole-mesh vmult on every owned entry within 1e-12 relative;
+* vmult equals the whole-mesh vmult on every owned entry within 1e-12
+  relative, for every caching variant and formulation;
 * the owned-entry dot product equals the whole-mesh one;
 * CG with the Jacobi preconditioner (diagonal summed across the interfaces)
   reaches the tolerance and its solution equals the whole-mesh CG solution
@@ -25,7 +28,7 @@ COARSE = (4, 4, 4)
 LEVEL = 1
 
 
-def _problem(n_parts, voids):
+def _problem(n_parts, voids, caching="tensor4", formulation=1):
     act = O.void_mask(COARSE, 3, 0.2, 5) if voids else None
     kw = dict(geometry="box", coarse=COARSE, n_refinements=LEVEL, degree=2, coarse_active=act)
     gm = lsmf.Mesh(**kw)
@@ -49,25 +52,29 @@ def _problem(n_parts, voids):
         owned[lay["upper_shared"]] = False
         od = (3 * np.nonzero(owned)[0][:, None] + np.arange(3)).reshape(-1)
         assert np.array_equal(pm.constraint_mask(), gm.constraint_mask()[gd])
-        op = lsmf.NeoHookOperator(pm, "tensor4", 1, "fp64")
+        op = lsmf.NeoHookOperator(pm, caching, formulation, "fp64")
         op.set_stream(torch.cuda.Stream())
         op.set_material(pmu, 0.3)
         du = torch.tensor(u[gd], device="cuda")
         op.cache(du)
         parts.append(dict(mesh=pm, op=op, u=du, gd=gd, od=od, lay=lay))
-    gop = lsmf.NeoHookOperator(gm, "tensor4", 1, "fp64")
+    gop = lsmf.NeoHookOperator(gm, caching, formulation, "fp64")
     gop.set_material(mu, 0.3)
     gu = torch.tensor(u, device="cuda")
     gop.cache(gu)
     return gm, gop, gu, parts, rng
 
 
+@pytest.mark.parametrize("exchange", ["packed", "fused"])
 @pytest.mark.parametrize("n_parts", [2, 3])
 @pytest.mark.parametrize("voids", [False, True])
-def test_group_vmult_dot_and_cg_equal_whole_mesh(n_parts, voids, parity):
+def test_group_vmult_dot_and_cg_equal_whole_mesh(n_parts, voids, exchange, parity):
     gm, gop, gu, parts, rng = _problem(n_parts, voids)
     nd = gm.info()[2]
     D = lsmf.Dist.group([p["op"] for p in parts])
+    assert D.exchange() == "fused"  # the default for parts on one GPU
+    D.set_exchange(exchange)
+    assert D.exchange() == exchange
     src = rng.uniform(-1, 1, nd)
     dsrc = torch.tensor(src, device="cuda")
     want = torch.empty_like(dsrc)
@@ -83,7 +90,7 @@ def test_group_vmult_dot_and_cg_equal_whole_mesh(n_parts, voids, parity):
     torch.cuda.synchronize()
     for p, d in zip(parts, dsts):
         got = d.cpu().numpy()
-        parity("partitioned vmult, %d parts%s" % (n_parts, ", voids" if voids else ""),
+        parity("partitioned vmult, %d parts%s, %s exchange" % (n_parts, ", voids" if voids else "", exchange),
                np.max(np.abs(got[p["od"]] - want[p["gd"][p["od"]]])) / np.max(np.abs(want)), 1e-12)
         assert np.max(np.abs(got[p["od"]] - want[p["gd"][p["od"]]])) <= 1e-12 * np.max(np.abs(want))
         # ghost entries of the result are cleared
@@ -115,6 +122,54 @@ def test_group_vmult_dot_and_cg_equal_whole_mesh(n_parts, voids, parity):
         assert np.max(np.abs(got - xg[p["gd"]])) <= 1e-9 * np.max(np.abs(xg))
 
 
+@pytest.mark.parametrize("caching,formulation", [("tensor2", 1), ("scalar", 1), ("scalar", 0),
+                                                  ("scalar_referential", 1), ("tensor4_ns", 1)])
+def test_fused_exchange_every_caching(caching, formulation, parity):
+    # the scalar variants also gather the displacement at the ghost nodes
+    # (from the owner's u in the fused form)
+    gm, gop, gu, parts, rng = _problem(3, True, caching, formulation)
+    nd = gm.info()[2]
+    src = rng.uniform(-1, 1, nd)
+    want = torch.empty(nd, dtype=torch.float64, device="cuda")
+    gop.vmult(want, torch.tensor(src, device="cuda"))
+    want = want.cpu().numpy()
+    D = lsmf.Dist.group([p["op"] for p in parts])
+    for exchange in ("fused", "packed"):
+        D.set_exchange(exchange)
+        srcs = [torch.tensor(src[p["gd"]], device="cuda") for p in parts]
+        dsts = [torch.full_like(s, 7.0) for s in srcs]
+        D.vmult(dsts, srcs)
+        torch.cuda.synchronize()
+        err = max(np.max(np.abs(d.cpu().numpy()[p["od"]] - want[p["gd"][p["od"]]])) for p, d in zip(parts, dsts))
+        parity("partitioned vmult, 3 parts, voids, %s f%d, %s exchange" % (caching, formulation, exchange),
+               err / np.max(np.abs(want)), 1e-12)
+        assert err <= 1e-12 * np.max(np.abs(want)), (exchange, err)
+
+
+def test_exchange_option():
+    gm, gop, gu, parts, rng = _problem(2, False)
+    D = lsmf.Dist.group([p["op"] for p in parts])
+    nd = gm.info()[2]
+    src = rng.uniform(-1, 1, nd)
+    want = torch.empty(nd, dtype=torch.float64, device="cuda")
+    gop.vmult(want, torch.tensor(src, device="cuda"))
+    want = want.cpu().numpy()
+    with pytest.raises(lsmf.LsmfError):
+        D.set_exchange(5)
+    # a deterministic scatter on one part: the vmult falls back to the packed
+    # exchange and stays right
+    parts[0]["op"].set_scatter("colour8")
+    assert D.exchange() == "packed"
+    srcs = [torch.tensor(src[p["gd"]], device="cuda") for p in parts]
+    dsts = [torch.empty_like(s) for s in srcs]
+    D.vmult(dsts, srcs)
+    torch.cuda.synchronize()
+    for p, d in zip(parts, dsts):
+        assert np.max(np.abs(d.cpu().numpy()[p["od"]] - want[p["gd"][p["od"]]])) <= 1e-12 * np.max(np.abs(want))
+    parts[0]["op"].set_scatter("atomic")
+    assert D.exchange() == "fused"
+
+
 def test_group_rejects_mismatched_parts():
     kw = dict(geometry="box", coarse=COARSE, n_refinements=LEVEL, degree=2)
     a = lsmf.Mesh(n_parts=2, part=0, **kw)
@@ -144,6 +199,11 @@ def test_nccl_transport_single_part():
     uid = lsmf.Dist.nccl_unique_id()
     assert len(uid) == 128
     D = lsmf.Dist.nccl(op, uid)
+    # one part per process: the interface data go through NCCL buffers
+    assert D.exchange() == "packed"
+    with pytest.raises(lsmf.LsmfError) as e:
+        D.set_exchange("fused")
+    assert e.value.status == 10  # LSMF_ERR_UNSUPPORTED
     src = torch.tensor(rng.uniform(-1, 1, nd), device="cuda")
     want, got = torch.empty_like(src), torch.empty_like(src)
     op.vmult(want, src)

@@ -128,3 +128,38 @@ def test_partitioned_vmult_equals_whole_mesh(world, voids):
         assert err < 1e-12, (r, err)
         assert abs(dot - dot_g) <= 1e-12 * abs(dot_g)
         assert once
+
+
+@pytest.mark.parametrize("world", [2, 3, 4])
+@pytest.mark.parametrize("voids", [False, True])
+def test_interface_lists_pair_the_same_nodes(world, voids):
+    """The fused exchange renumbers part r's ghost nodes (upper_shared[j])
+    as part r + 1's nodes lower_shared[j]: both lists must name the same
+    whole-mesh nodes in the same order, within each part's node range and
+    below the peer bit (2^28) of the index map, and the ghosts must lie on
+    the part's top node plane."""
+    import lsmf
+    act = _mask(voids)
+    lays = [lsmf.partition_layout(world, r, geometry="box", coarse=COARSE, n_refinements=LEVEL, degree=2,
+                                  coarse_active=act) for r in range(world)]
+    for r in range(world):
+        lay = lays[r]
+        n = lay["n_nodes"]
+        assert n < 2 ** 28
+        for lst in (lay["lower_shared"], lay["upper_shared"]):
+            assert lst.size == 0 or (lst.min() >= 0 and lst.max() < n)
+        if r + 1 < world:
+            up, lo = lay["upper_shared"], lays[r + 1]["lower_shared"]
+            assert up.size == lo.size > 0
+            assert np.array_equal(lay["global_node"][up], lays[r + 1]["global_node"][lo])
+        else:
+            assert lay["upper_shared"].size == 0
+        if r == 0:
+            assert lay["lower_shared"].size == 0
+    # ghosts sit on the part's top plane z = k1 / nz (whole-mesh coordinates
+    # from the oracle's mesh; node numbers are compacted around voids)
+    import oracle as O
+    og = O.Mesh(O.GEOM_BOX, COARSE, LEVEL, (0, 0, 0), (1, 1, 1), 1.0, 2, 3, coarse_active=act)
+    for r in range(world - 1):
+        z = og.X[lays[r]["global_node"][lays[r]["upper_shared"]], 2]
+        assert np.max(np.abs(z - (COARSE[2] * (r + 1) // world) / COARSE[2])) < 1e-14
