@@ -923,10 +923,14 @@ def run_lsmf(args):
     alg = alg_bytes("tensor4", 8, n_nodes, n_qp, n_cells)
     achieved = alg / (apply_ms * 1e-3) / 1e9
     traffic = read_traffic()
+    chunks = op.get_option(8)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "peak_kind": peak_kind, "alg_bytes_per_launch": alg,
-                "kernel": "apply_fast_kernel<2,3,double,tensor4,1 stage>"}
+                "kernel": "apply_fast_kernel<2,3,double,tensor4,1 stage>",
+                "chunks": chunks,
+                "timed": "the cell loop of one vmult_add (its %d concurrent chunks forked from and joined back into "
+                         "the timing stream) plus the identity rows, CUDA events on that stream" % chunks}
 
     # MFMask stage breakdown (RW / SF / QD) of the FP64 variants
     stages = {}
@@ -978,7 +982,9 @@ def run_lsmf(args):
                            "parallelism": "replicas" if world > 1 else "single GPU",
                            "l2": "inputs larger than L2 (2.9 GB cache tables), no flush"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": 2 * args.steps, "clocks": clocks, "variants": variants,
+                # per vmult: one apply launch per chunk and one identity-row
+                # launch (the clamped bottom face lies in the first chunk)
+                "gpu_launches": (chunks + 1) * args.steps, "clocks": clocks, "variants": variants,
                 "stage_split_fp64": stages, "large_vmults": large, "dist_vmult_one_gpu": dist_parts,
                 "newton_step": newton, "newton_load_steps": load_steps, "adjoint": adjoint}
         print(json.dumps(line), flush=True)

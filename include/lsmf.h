@@ -174,13 +174,29 @@ lsmf_status lsmf_operator_el(lsmf_op *op, int row, int col, double *value);
  *   measured choice (pairs for Q1 tensor2 / scalar formulation 1, Q2
  *   tensor2 / scalar formulation 1 / scalar_referential, Q4
  *   scalar_referential).  Ignored for FP64 operators.
+ * LSMF_OPT_CHUNKS: the atomic-scatter vmult cell loop split into 2..8
+ *   contiguous cell chunks on streams of the operator's own, forked from
+ *   and joined back into its stream: each chunk zeroes its range of dst and
+ *   applies the identity rows there, then runs its cells once the next
+ *   chunk has zeroed its range, so the zeroing, the identity rows and the
+ *   ends of the chunks' launches overlap other chunks' cell loops (levels
+ *   with fewer than 1024 cells per chunk run in one piece); 1 = one launch;
+ *   -1 (default) = measured choice: from 131,072 cells 8 for
+ *   scalar_referential and tensor4_ns, 2 for tensor2, 4 otherwise; from
+ *   32,768 cells 2; below that 1.  The operators a GMG object or a problem
+ *   creates start at 1 (measured faster inside the Newton solve).
  * A bounded device wait that runs out in the pipelined kernel is reported
  * as LSMF_ERR_TIMEOUT by lsmf_operator_sync, lsmf_cg_solve and the GMG
  * set-up (the next synchronising call on the operator). */
 enum { LSMF_OPT_BULK_PIPELINE = 1, LSMF_OPT_BASIC_KERNEL = 2, LSMF_OPT_MAX_WARPS = 3, LSMF_OPT_WAIT_TRIES = 4,
-       LSMF_OPT_SCATTER = 5, LSMF_OPT_RECORD_PREFETCH = 6, LSMF_OPT_CELL_PAIRS = 7 };
+       LSMF_OPT_SCATTER = 5, LSMF_OPT_RECORD_PREFETCH = 6, LSMF_OPT_CELL_PAIRS = 7, LSMF_OPT_CHUNKS = 8 };
 enum { LSMF_SCATTER_ATOMIC = 0, LSMF_SCATTER_COLOUR8 = 1, LSMF_SCATTER_NODESUM = 2 };
 lsmf_status lsmf_operator_set_option(lsmf_op *op, int option, int value);
+/* The value of an option as set (-1 / 0 for the automatic choices), except
+ * LSMF_OPT_CHUNKS, which reports the chunk count the next full vmult cell
+ * loop runs in (the automatic choice resolved; 1 = one launch).  No
+ * reference counterpart. */
+lsmf_status lsmf_operator_get_option(lsmf_op *op, int option, int *value);
 /* Wait for the operator's stream and report a device error its kernels
  * recorded since the last report (LSMF_ERR_TIMEOUT for a bounded wait that
  * ran out; the word is cleared once reported).  No reference counterpart:

@@ -251,7 +251,28 @@ lsmf_status lsmf_operator_set_option(lsmf_op *op, int option, int value) {
     op->pairs = value;
     return LSMF_OK;
   }
+  if (option == LSMF_OPT_CHUNKS) {
+    if (value < -1 || value == 0 || value > 8) { set_error("chunks must be -1 (auto) or 1..8"); return LSMF_ERR_INVALID_ARG; }
+    op->chunks = value;
+    return LSMF_OK;
+  }
   if (option == LSMF_OPT_SCATTER) return set_scatter_mode(op, value);
+  set_error("unknown option");
+  return LSMF_ERR_INVALID_ARG;
+}
+
+lsmf_status lsmf_operator_get_option(lsmf_op *op, int option, int *value) {
+  if (!op || !value) { set_error("null argument"); return LSMF_ERR_INVALID_ARG; }
+  switch (option) {
+    case LSMF_OPT_BULK_PIPELINE: *value = op->stages; return LSMF_OK;
+    case LSMF_OPT_BASIC_KERNEL: *value = op->basic ? 1 : 0; return LSMF_OK;
+    case LSMF_OPT_MAX_WARPS: *value = op->max_warps; return LSMF_OK;
+    case LSMF_OPT_WAIT_TRIES: *value = op->wait_tries; return LSMF_OK;
+    case LSMF_OPT_SCATTER: *value = op->scatter; return LSMF_OK;
+    case LSMF_OPT_RECORD_PREFETCH: *value = op->prefetch; return LSMF_OK;
+    case LSMF_OPT_CELL_PAIRS: *value = op->pairs; return LSMF_OK;
+    case LSMF_OPT_CHUNKS: return effective_chunks(op, value);
+  }
   set_error("unknown option");
   return LSMF_ERR_INVALID_ARG;
 }

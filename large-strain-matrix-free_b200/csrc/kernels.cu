@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include "cell_kernels.cuh"
@@ -184,6 +185,139 @@ lsmf_status set_scatter_mode(lsmf_op *op, int mode) {
   return LSMF_OK;
 }
 
+// Chunks of an operator's atomic-scatter cell loop: the option, or the
+// measured choice.  Swept on B200 over 1 / 2 / 4 / 6 / 8 chunks for every
+// variant and precision at 64^3 Q2 and for tensor4 at 32^3 / 40^3 Q2 and
+// 48^3 Q3 / Q4 (vmult time against one launch): from 131,072 cells 8 for
+// the referential variants (scalar_referential FP64 -7 %, tensor4_ns FP64 /
+// FP32 -4 / -6 %), 2 for tensor2 (-1 / -2 %), 4 for the others (tensor4
+// FP64 / FP32 -3.5 / -4 %, scalar -2 %); from 32,768 cells 2 (32^3 Q2
+// tensor4 FP64 / FP32 -4.5 / -10 %, 48^3 Q3 / Q4 under -1 %); fewer cells
+// run in one launch.
+static int chunk_count(const lsmf_op *op) {
+  if (op->chunks > 0) return op->chunks;
+  const int n = op->L().n_cells;
+  if (n >= 131072) {
+    if (op->caching == LSMF_CACHE_TENSOR4_NS || op->caching == LSMF_CACHE_SCALAR_REFERENTIAL) return 8;
+    return op->caching == LSMF_CACHE_TENSOR2 ? 2 : 4;
+  }
+  return n >= 32768 ? 2 : 1;
+}
+
+// The operator's plan for k chunks (*out = nullptr where it does not apply:
+// k < 2, fewer than 1024 cells per chunk, or a chunk whose cells reach past
+// the next chunk's node range).  Cells and nodes are numbered z-slowest, so
+// contiguous cell chunks touch nearly contiguous node ranges; chunk c owns
+// the nodes from the lowest one its cells touch up to the next chunk's.
+static lsmf_status chunk_plan(const lsmf_op *op, int k, const ChunkPlan **out) {
+  *out = nullptr;
+  if (k < 2) return LSMF_OK;
+  if (op->chunk_plan && op->chunk_plan->requested == k) {
+    if (op->chunk_plan->k) *out = op->chunk_plan.get();
+    return LSMF_OK;
+  }
+  auto plan = std::make_unique<ChunkPlan>();
+  plan->requested = k;
+  const Level &L = op->L();
+  const int ncn = L.ncn();
+  bool ok = k <= 8 && L.n_cells >= 1024 * k;
+  if (ok) {
+    plan->cell0.resize(k + 1);
+    plan->node0.resize(k + 1);
+    std::vector<int> nmax(k);
+    for (int c = 0; c <= k; ++c) plan->cell0[c] = (int)((long long)L.n_cells * c / k);
+    for (int c = 0; c < k; ++c) {
+      int lo = L.n_nodes, hi = -1;
+      for (size_t i = (size_t)plan->cell0[c] * ncn; i < (size_t)plan->cell0[c + 1] * ncn; ++i) {
+        lo = std::min(lo, L.cell_nodes[i]);
+        hi = std::max(hi, L.cell_nodes[i]);
+      }
+      plan->node0[c] = c == 0 ? 0 : lo;
+      nmax[c] = hi;
+    }
+    plan->node0[k] = L.n_nodes;
+    for (int c = 0; c < k && ok; ++c) {
+      ok = plan->node0[c] <= plan->node0[c + 1];
+      if (c + 2 <= k) ok = ok && nmax[c] < plan->node0[c + 2];
+    }
+  }
+  if (ok) {
+    for (int c = 0; c < k; ++c) {
+      LSMF_CUDA(cudaStreamCreateWithFlags(&plan->stream[c], cudaStreamNonBlocking));
+      LSMF_CUDA(cudaEventCreateWithFlags(&plan->zero[c], cudaEventDisableTiming));
+      LSMF_CUDA(cudaEventCreateWithFlags(&plan->done[c], cudaEventDisableTiming));
+    }
+    LSMF_CUDA(cudaEventCreateWithFlags(&plan->fork, cudaEventDisableTiming));
+    plan->k = k;
+  }
+  op->chunk_plan = std::move(plan);
+  if (op->chunk_plan->k) *out = op->chunk_plan.get();
+  return LSMF_OK;
+}
+
+// the chunked path applies: atomic scatter, fast kernels, the full cell loop
+static bool chunkable(const lsmf_op *op, unsigned mask) {
+  const unsigned all = LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD;
+  return op->scatter == LSMF_SCATTER_ATOMIC && !op->basic && (mask & all) == all && !(mask & MASK_INHOM_BIT);
+}
+
+// chunks the operator's next full vmult cell loop runs in (1: one launch)
+lsmf_status effective_chunks(const lsmf_op *op, int *k) {
+  *k = 1;
+  if (!chunkable(op, LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD)) return LSMF_OK;
+  const ChunkPlan *cp = nullptr;
+  LSMF_TRY(chunk_plan(op, chunk_count(op), &cp));
+  if (cp) *k = cp->k;
+  return LSMF_OK;
+}
+
+
+// The vmult over the plan's chunks, forked from and joined back into the
+// operator's stream: chunk c zeroes its node range of dst (zero) and adds
+// the identity rows of the constrained dofs in it (rows), then runs its
+// cells once chunk c + 1 has zeroed its range (its cells add into that
+// range's first node layer).  The scatter skips constrained components, so
+// the identity rows are never touched by another chunk.
+static lsmf_status apply_chunked(const lsmf_op *op, const OpsTable *t, const ChunkPlan &cp, void *dst,
+                                 const void *src, unsigned mask, bool zero, bool rows) {
+  const Level &L = op->L();
+  const size_t e = op->elem();
+  const int g_max = 4 * num_sms();
+  LSMF_CUDA(cudaEventRecord(cp.fork, op->stream));
+  for (int c = 0; c < cp.k; ++c) {
+    cudaStream_t st = cp.stream[c];
+    LSMF_CUDA(cudaStreamWaitEvent(st, cp.fork, 0));
+    const size_t d0 = 3 * (size_t)cp.node0[c], d1 = 3 * (size_t)cp.node0[c + 1];
+    if (zero && d1 > d0) LSMF_CUDA(cudaMemsetAsync((char *)dst + d0 * e, 0, (d1 - d0) * e, st));
+    if (rows) {
+      // L.constrained is in increasing dof order
+      const int a0 = (int)(std::lower_bound(L.constrained.begin(), L.constrained.end(), (int)d0) - L.constrained.begin());
+      const int a1 = (int)(std::lower_bound(L.constrained.begin(), L.constrained.end(), (int)d1) - L.constrained.begin());
+      const int nc = a1 - a0;
+      if (nc > 0) {
+        const int g = (nc + 255) / 256 < g_max ? (nc + 255) / 256 : g_max;
+        if (op->precision == LSMF_FP64)
+          constrained_add_kernel<double><<<g, 256, 0, st>>>((double *)dst, (const double *)src, L.d_constrained.ptr + a0, nc);
+        else
+          constrained_add_kernel<float><<<g, 256, 0, st>>>((float *)dst, (const float *)src, L.d_constrained.ptr + a0, nc);
+        LSMF_CUDA(cudaGetLastError());
+      }
+    }
+    LSMF_CUDA(cudaEventRecord(cp.zero[c], st));
+  }
+  for (int c = 0; c < cp.k; ++c) {
+    if (c + 1 < cp.k) LSMF_CUDA(cudaStreamWaitEvent(cp.stream[c], cp.zero[c + 1], 0));
+    CellRange r;
+    r.first = cp.cell0[c];
+    r.count = cp.cell0[c + 1] - cp.cell0[c];
+    r.stream = cp.stream[c];
+    LSMF_TRY(t->apply(op, dst, src, mask, r));
+    LSMF_CUDA(cudaEventRecord(cp.done[c], cp.stream[c]));
+  }
+  for (int c = 0; c < cp.k; ++c) LSMF_CUDA(cudaStreamWaitEvent(op->stream, cp.done[c], 0));
+  return LSMF_OK;
+}
+
 lsmf_status launch_apply(const lsmf_op *op, void *dst, const void *src, unsigned mask, bool add) {
   const Level &L = op->L();
   const OpsTable *t = table_of(op);
@@ -192,6 +326,11 @@ lsmf_status launch_apply(const lsmf_op *op, void *dst, const void *src, unsigned
   if (node_sum_path(op, mask)) {
     LSMF_TRY(apply_node_sum(op, t, dst, src, mask, add || !(mask & LSMF_MASK_ZERO)));
   } else {
+    if (chunkable(op, mask)) {
+      const ChunkPlan *cp = nullptr;
+      LSMF_TRY(chunk_plan(op, chunk_count(op), &cp));
+      if (cp) return apply_chunked(op, t, *cp, dst, src, mask, !add && (mask & LSMF_MASK_ZERO), true);
+    }
     if (!add && (mask & LSMF_MASK_ZERO)) LSMF_CUDA(cudaMemsetAsync(dst, 0, n * op->elem(), op->stream));
     LSMF_TRY(for_cell_ranges(L, op->scatter, [&](CellRange r) { return t->apply(op, dst, src, mask, r); }));
   }
@@ -236,6 +375,25 @@ lsmf_status launch_apply_cells(const lsmf_op *op, void *dst, const void *src) {
   if (!t) return LSMF_ERR_UNSUPPORTED;
   const unsigned mask = LSMF_MASK_RW | LSMF_MASK_SF | LSMF_MASK_QD;
   if (node_sum_path(op, mask)) return apply_node_sum(op, t, dst, src, mask, true);
+  if (chunkable(op, mask)) {
+    // the chunks' cell loops only, concurrent (nothing to zero)
+    const ChunkPlan *cp = nullptr;
+    LSMF_TRY(chunk_plan(op, chunk_count(op), &cp));
+    if (cp) {
+      LSMF_CUDA(cudaEventRecord(cp->fork, op->stream));
+      for (int c = 0; c < cp->k; ++c) {
+        LSMF_CUDA(cudaStreamWaitEvent(cp->stream[c], cp->fork, 0));
+        CellRange r;
+        r.first = cp->cell0[c];
+        r.count = cp->cell0[c + 1] - cp->cell0[c];
+        r.stream = cp->stream[c];
+        LSMF_TRY(t->apply(op, dst, src, mask, r));
+        LSMF_CUDA(cudaEventRecord(cp->done[c], cp->stream[c]));
+      }
+      for (int c = 0; c < cp->k; ++c) LSMF_CUDA(cudaStreamWaitEvent(op->stream, cp->done[c], 0));
+      return LSMF_OK;
+    }
+  }
   return for_cell_ranges(op->L(), op->scatter, [&](CellRange r) { return t->apply(op, dst, src, mask, r); });
 }
 

@@ -10,6 +10,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <memory>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -183,6 +184,29 @@ struct lsmf_mesh {
   ~lsmf_mesh();
 };
 
+namespace lsmf {
+// The vmult cell loop of a large level split into k contiguous cell chunks
+// on concurrent streams (kernels.cu).  Chunk c zeroes the dst node range
+// node0[c] .. node0[c+1] (every node its cells touch lies in its own or the
+// next chunk's range), applies the identity rows of the constrained dofs
+// there, then runs its cell loop once chunk c + 1 has zeroed its range.
+struct ChunkPlan {
+  int requested = 0;                 // chunk count asked for
+  int k = 0;                         // 0: the plan does not apply to this level
+  std::vector<int> cell0, node0;     // k + 1 offsets
+  cudaStream_t stream[8] = {};
+  cudaEvent_t fork = nullptr, zero[8] = {}, done[8] = {};
+  ~ChunkPlan() {
+    for (int c = 0; c < 8; ++c) {
+      if (stream[c]) cudaStreamDestroy(stream[c]);
+      if (zero[c]) cudaEventDestroy(zero[c]);
+      if (done[c]) cudaEventDestroy(done[c]);
+    }
+    if (fork) cudaEventDestroy(fork);
+  }
+};
+}  // namespace lsmf
+
 struct lsmf_op {
   lsmf_mesh *mesh = nullptr;
   int level = 0;
@@ -208,6 +232,10 @@ struct lsmf_op {
   int device = 0;                    // CUDA device the operator's buffers live on
   int scatter = LSMF_SCATTER_ATOMIC; // cell-loop scatter: atomics, the 8 colour launches, or node sums
   lsmf::DevBuf<char> d_cellbuf;      // node-sum scatter: per-cell results [cell][local node][component]
+  // concurrent chunks of the atomic-scatter vmult cell loop (-1 auto, 1 off,
+  // 2..8); the plan for the chosen count is built on first use
+  int chunks = -1;
+  mutable std::unique_ptr<lsmf::ChunkPlan> chunk_plan;
   cudaStream_t stream = 0;
   // CG workspace (outer FP64 CG driven through this operator)
   lsmf::DevBuf<double> cg_g, cg_h, cg_d, sc, partial;
@@ -227,6 +255,8 @@ lsmf_status launch_diagonal(lsmf_op *op);
 // node-sum mode builds the level's node -> cell lists and the operator's
 // cell buffer on first use
 lsmf_status set_scatter_mode(lsmf_op *op, int mode);
+// chunks the operator's next full vmult cell loop runs in (1: one launch)
+lsmf_status effective_chunks(const lsmf_op *op, int *k);
 lsmf_status upload_basis_tables(const Basis &b);
 int table_components(int caching, int formulation, lsmf_precision precision);
 }  // namespace lsmf

@@ -25,6 +25,11 @@ struct CellRange {
   const void *peer_src = nullptr;
   void *peer_dst = nullptr;
   const void *peer_u = nullptr;
+  // contiguous cells first .. first + count - 1 of the level (count >= 0,
+  // atomic scatter), launched on `stream` (nullptr: the operator's stream):
+  // one chunk of a cell loop split over concurrent streams
+  int first = 0, count = -1;
+  cudaStream_t stream = nullptr;
 };
 
 struct OpsTable {

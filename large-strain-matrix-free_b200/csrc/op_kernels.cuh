@@ -50,11 +50,12 @@ struct KArgs {
   const T *psrc;
   T *pdst;
   const T *pu;
+  int cell0;             // first cell of a contiguous chunk (cell list absent)
 };
 
 // cell of list entry i
 template <typename T>
-__device__ __forceinline__ int cell_of(const KArgs<T> &a, int i) { return a.cells ? __ldg(a.cells + i) : i; }
+__device__ __forceinline__ int cell_of(const KArgs<T> &a, int i) { return a.cells ? __ldg(a.cells + i) : a.cell0 + i; }
 template <typename T>
 __device__ __forceinline__ void scatter_add(T *p, T v, bool plain) {
   if (plain) *p += v;
@@ -448,7 +449,7 @@ __global__ void __launch_bounds__(256) apply_fast_kernel(KArgs<T> a, TabT<P, Q, 
   T *slab = (T *)(wbase + STAGES * rec_bytes + 8 * NS);
   const int gw = blockIdx.x * WPB + warp, nw = gridDim.x * WPB;
   // list entry -> cell
-  auto cid = [&](int i) -> int { return COL ? __ldg(a.cells + i) : i; };
+  auto cid = [&](int i) -> int { return COL ? __ldg(a.cells + i) : a.cell0 + i; };
   uint64_t pol = 0;
   if (STAGES > 0) {
     pol = evict_first_policy();
@@ -699,7 +700,7 @@ __global__ void __launch_bounds__(256) apply_pair_kernel(KArgs<float> a, TabT<P,
   T *slab = (T *)(smem + warp * warp_bytes + 8);
   const int gw = blockIdx.x * WPB + warp, nw = gridDim.x * WPB;
   const int n_pairs = (a.n_cells + 1) >> 1;
-  auto cid = [&](int i) -> int { return COL ? __ldg(a.cells + i) : i; };
+  auto cid = [&](int i) -> int { return COL ? __ldg(a.cells + i) : a.cell0 + i; };
   // gather registers of the x rows (c, k, j) owned by this lane, both cells
   int pk0[RPL][N1], pk1[RPL][N1];
   float pv0[RPL][N1], pv1[RPL][N1], pu0[RPL][N1], pu1[RPL][N1];
@@ -1077,6 +1078,7 @@ KArgs<T> make_args(const lsmf_op *op) {
   a.psrc = nullptr;
   a.pdst = nullptr;
   a.pu = nullptr;
+  a.cell0 = 0;
   return a;
 }
 
@@ -1088,6 +1090,10 @@ void set_range(KArgs<T> &a, const CellRange &r) {
   }
   a.plain = r.plain ? 1 : 0;
   a.cellbuf = (T *)r.cellbuf;
+  if (r.count >= 0) {
+    a.cell0 = r.first;
+    a.n_cells = r.count;
+  }
   if (r.peer_nodes) {
     a.cell_nodes = r.peer_nodes;
     a.psrc = (const T *)r.peer_src;
@@ -1114,6 +1120,7 @@ lsmf_status run_cache(lsmf_op *op) {
 template <int P, int Q, typename T, int VAR>
 lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, CellRange range) {
   auto a = make_args<T>(op);
+  cudaStream_t stream = range.stream ? range.stream : op->stream;
   a.src = src;
   a.dst = dst;
   a.mask = mask;
@@ -1202,7 +1209,7 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
       auto go = [&](auto k) -> lsmf_status {
         LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_p));
         const int g = grid_for(k, 32 * w, smem_p, (n_pairs + w - 1) / w);
-        k<<<g, 32 * w, smem_p, op->stream>>>(a, tabp);
+        k<<<g, 32 * w, smem_p, stream>>>(a, tabp);
         return LSMF_OK;
       };
       if (col) return go(apply_pair_kernel<P, Q, VAR, SC_COLOUR>);
@@ -1219,7 +1226,7 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
     auto go = [&](auto k) -> lsmf_status {
       LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t));
       const int g = grid_for(k, 32 * w, smem_t, (a.n_cells + w - 1) / w);
-      k<<<g, 32 * w, smem_t, op->stream>>>(a, tabt);
+      k<<<g, 32 * w, smem_t, stream>>>(a, tabt);
       return LSMF_OK;
     };
     if (col) {
@@ -1245,12 +1252,12 @@ lsmf_status run_apply(const lsmf_op *op, T *dst, const T *src, unsigned mask, Ce
     auto k = apply_kernel<P, Q, T, VAR, true>;
     LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int g = grid_for(k, 32 * w, smem, (a.n_cells + w - 1) / w);
-    k<<<g, 32 * w, smem, op->stream>>>(a, tab);
+    k<<<g, 32 * w, smem, stream>>>(a, tab);
   } else {
     auto k = apply_kernel<P, Q, T, VAR, false>;
     LSMF_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int g = grid_for(k, 32 * w, smem, (a.n_cells + w - 1) / w);
-    k<<<g, 32 * w, smem, op->stream>>>(a, tab);
+    k<<<g, 32 * w, smem, stream>>>(a, tab);
   }
   LSMF_CUDA(cudaGetLastError());
   return LSMF_OK;

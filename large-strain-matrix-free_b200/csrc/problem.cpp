@@ -494,6 +494,11 @@ lsmf_status lsmf_problem_create(const char *text, lsmf_problem **out) {
     delete pb;
     return s;
   }
+  // the Newton driver's operator in one launch: with its cell loop chunked
+  // the Newton step of the voids benchmark (60^3 Q2, FP32 and FP64 levels)
+  // measured 3.5-4.5 % slower, although the chunked operator alone and in a
+  // Jacobi-CG measured faster
+  pb->op->chunks = 1;
   if (precond_code(P.precond) == 2) {
     lsmf_gmg_desc gd{};
     gd.caching = caching;

@@ -119,6 +119,7 @@ SIGNATURES = {
     "lsmf_dist_create_nccl": (ctypes.c_int, [vp, vp, ctypes.POINTER(vp)]),
     "lsmf_dist_destroy": (None, [vp]),
     "lsmf_dist_vmult": (ctypes.c_int, [vp, vp, vp]),
+    "lsmf_operator_get_option": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "lsmf_dist_set_exchange": (ctypes.c_int, [vp, ctypes.c_int]),
     "lsmf_dist_get_exchange": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int)]),
     "lsmf_dist_dot": (ctypes.c_int, [vp, vp, vp, dp]),
@@ -359,6 +360,19 @@ class NeoHookOperator:
         tensor2 / scalar, Q2 tensor2 / scalar / scalar_referential, Q4
         scalar_referential; formulation 1)."""
         check(lib().lsmf_operator_set_option(self.h, 7, int(mode)))
+
+    def set_chunks(self, k):
+        """Atomic-scatter vmult cell loop in k (2..8) concurrent cell chunks,
+        each zeroing its own range of dst first; 1 = one launch, -1 = the
+        measured default."""
+        check(lib().lsmf_operator_set_option(self.h, 8, int(k)))
+
+    def get_option(self, option):
+        """lsmf_operator_get_option: the option as set; for 8 (chunks) the
+        chunk count the next vmult cell loop runs in."""
+        v = ctypes.c_int()
+        check(lib().lsmf_operator_get_option(self.h, int(option), ctypes.byref(v)))
+        return v.value
 
     def sync(self):
         """Wait for the operator's stream; raises LsmfError (status 8) if a
