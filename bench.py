@@ -919,6 +919,9 @@ def run_lsmf(args):
            "frac_of_link": round(link_ms / e2e_ms, 3),
            "link_definition": "the step's H2D and D2H copies run concurrently without the vmult (measured here)"}
     lib.lsmf_operator_set_stream(op.h, lsmf.vp(stream.cuda_stream))
+    # release the section's pinned buffers, device vectors and streams
+    torch.cuda.synchronize()
+    del src_pin, dst_pin, d_src, d_dst, s_h2d, s_d2h, s_cmp, ev_in, ev_done, ev_out
 
     alg = alg_bytes("tensor4", 8, n_nodes, n_qp, n_cells)
     achieved = alg / (apply_ms * 1e-3) / 1e9
