@@ -184,7 +184,9 @@ lsmf_status lsmf_operator_el(lsmf_op *op, int row, int col, double *value);
  *   -1 (default) = measured choice: from 131,072 cells 8 for
  *   scalar_referential and tensor4_ns, 2 for tensor2, 4 otherwise; from
  *   32,768 cells 2; below that 1.  The operators a GMG object or a problem
- *   creates start at 1 (measured faster inside the Newton solve).
+ *   creates start at 1 (measured faster inside the Newton solve).  The
+ *   chunks' streams and events are created by lsmf_operator_cache (and by
+ *   this option on a cached operator), not by the vmult.
  * A bounded device wait that runs out in the pipelined kernel is reported
  * as LSMF_ERR_TIMEOUT by lsmf_operator_sync, lsmf_cg_solve and the GMG
  * set-up (the next synchronising call on the operator). */

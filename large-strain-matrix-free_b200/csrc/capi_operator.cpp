@@ -254,7 +254,10 @@ lsmf_status lsmf_operator_set_option(lsmf_op *op, int option, int value) {
   if (option == LSMF_OPT_CHUNKS) {
     if (value < -1 || value == 0 || value > 8) { set_error("chunks must be -1 (auto) or 1..8"); return LSMF_ERR_INVALID_ARG; }
     op->chunks = value;
-    return LSMF_OK;
+    // a cached operator builds the plan for the new count now, not inside
+    // the first vmult (which may run in a stream capture)
+    int k = 1;
+    return op->cached ? effective_chunks(op, &k) : LSMF_OK;
   }
   if (option == LSMF_OPT_SCATTER) return set_scatter_mode(op, value);
   set_error("unknown option");
@@ -297,7 +300,10 @@ lsmf_status lsmf_operator_cache(lsmf_op *op, const void *d_u) {
     return LSMF_ERR_DETF_NONPOSITIVE;
   }
   op->cached = true;
-  return LSMF_OK;
+  // the chunk plan of the vmult (streams, events, node ranges) is built
+  // here, outside any stream capture a caller may later run the vmult in
+  int k = 1;
+  return effective_chunks(op, &k);
 }
 
 lsmf_status lsmf_operator_vmult(lsmf_op *op, void *d_dst, const void *d_src, unsigned mask) {
