@@ -132,6 +132,18 @@ def test_multigrid_levels_start_unchunked():
     assert v.value == 2
 
 
+def test_get_option_reports_what_was_set():
+    gm = _mesh(2, (2, 2, 2), 1)
+    op, src = _op(gm, "tensor4", 1, "fp32")
+    for opt, val in ((1, 2), (2, 1), (3, 6), (4, 1000), (6, 0), (7, 1)):
+        lsmf.lib().lsmf_operator_set_option(op.h, opt, val)
+        assert op.get_option(opt) == val, opt
+    op.set_scatter("nodesum")
+    assert op.get_option(5) == 2
+    with pytest.raises(lsmf.LsmfError):
+        op.get_option(99)
+
+
 def test_option_validation():
     gm = _mesh(2, (2, 2, 2), 1)
     op, src = _op(gm, "tensor4", 1, "fp64")
