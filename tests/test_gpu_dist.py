@@ -146,6 +146,29 @@ def test_fused_exchange_every_caching(caching, formulation, parity):
         assert err <= 1e-12 * np.max(np.abs(want)), (exchange, err)
 
 
+def test_fused_exchange_parts_on_one_stream():
+    # parts left on the default stream: every zeroing, wait and cell loop of
+    # the fused exchange is ordered on the same stream (each wait follows its
+    # event's record in that order)
+    gm, gop, gu, parts, rng = _problem(3, True)
+    for p in parts:
+        p["op"].set_stream(None)
+    nd = gm.info()[2]
+    src = rng.uniform(-1, 1, nd)
+    want = torch.empty(nd, dtype=torch.float64, device="cuda")
+    gop.vmult(want, torch.tensor(src, device="cuda"))
+    want = want.cpu().numpy()
+    D = lsmf.Dist.group([p["op"] for p in parts])
+    assert D.exchange() == "fused"
+    srcs = [torch.tensor(src[p["gd"]], device="cuda") for p in parts]
+    dsts = [torch.empty_like(s) for s in srcs]
+    for _ in range(2):
+        D.vmult(dsts, srcs)
+    torch.cuda.synchronize()
+    for p, d in zip(parts, dsts):
+        assert np.max(np.abs(d.cpu().numpy()[p["od"]] - want[p["gd"][p["od"]]])) <= 1e-12 * np.max(np.abs(want))
+
+
 def test_exchange_option():
     gm, gop, gu, parts, rng = _problem(2, False)
     D = lsmf.Dist.group([p["op"] for p in parts])
